@@ -1,0 +1,809 @@
+/*
+ * bes_kernel.cuh -- the persistent ensemble integrator for sm_100a.
+ *
+ * One warp integrates one system; lane l owns units l, l+32, ..., l+32(U-1)
+ * (U = 1, 2, 4 for N <= 32, 64, 128).  Warps pull systems from a global work
+ * counter until the ensemble is done, and each system runs `n_periods`
+ * consecutive reference Solve() calls inside the one launch.
+ *
+ * Reference behaviour restated here (file:line in the reference):
+ *   step loop, callbacks, write-back  SourceCodes/CoupledSystmes_PerBlock_Solver.cuh:82-648
+ *   RKCK45 stages, y5, error          SourceCodes/CoupledSystems_PerBlock_ExplicitRungeKutta_Steppers.cuh:94-425
+ *   BiCG for the coupled accelerations ...ExplicitRungeKutta_Steppers.cuh:432-562, helpers :565-805
+ *   step-size controller              SourceCodes/CoupledSystems_PerBlock_ExplicitRungeKutta_ErrorControllers.cuh:454-542
+ *   RK4 fixed-step controller         ...ExplicitRungeKutta_ErrorControllers.cuh:424-450
+ *   event step cut                    SourceCodes/CoupledSystems_PerBlock_EventHandling.cuh:216-268
+ *   dense output                      SourceCodes/CoupledSystems_PerBlock_DenseOutput.cuh:312-395
+ *
+ * B200 design: the reference's shared-memory tree reductions and CAS
+ * atomics become warp butterflies (the butterfly computes the reference's
+ * halving-tree sum exactly, because IEEE addition is commutative); the
+ * transposed product A^T p~, which the reference forms with N block-wide
+ * reductions per BiCG iteration, becomes one column tree per lane over the
+ * operator W_ij = (rD_i C_ij) X0_j^2 that is formed once per right-hand side
+ * in shared memory (leading dimension 32U+1: conflict-free row and column
+ * reads).  Every scalar of the step control is warp-uniform and held in
+ * registers, so a step needs no block barrier at all.
+ *
+ * Arithmetic order (identical in the CPU oracle): sums over units are the
+ * halving tree over units padded with zeros to 32U; the row products
+ * accumulate columns 0..N-1 with fma; every fused multiply-add is explicit
+ * (the file is compiled with --fmad=false).
+ */
+#ifndef BES_KERNEL_CUH
+#define BES_KERNEL_CUH
+
+#include "bes_device.h"
+#include "bes_math.cuh"
+#include "bes_status.h"
+
+#ifndef BES_SYSTEM_DEFINITION
+#include "km_model.cuh"
+#else
+#include BES_SYSTEM_DEFINITION
+#endif
+
+namespace bes {
+
+constexpr int UD = BES_MODEL_UD;
+constexpr int NUP = BES_MODEL_NUP;
+constexpr int NUA = BES_MODEL_NUA;
+constexpr int NIUA = BES_MODEL_NIUA;
+constexpr int NE = BES_MODEL_NE;
+constexpr int NSP = BES_MODEL_NSP;
+constexpr int NSA = BES_MODEL_NSA;
+constexpr int NISA = BES_MODEL_NISA;
+constexpr int IC = BES_MODEL_IMPLICIT_COMPONENT;
+constexpr int NUPa = NUP > 0 ? NUP : 1;
+constexpr int NUAa = NUA > 0 ? NUA : 1;
+constexpr int NIUAa = NIUA > 0 ? NIUA : 1;
+constexpr int NEa = NE > 0 ? NE : 1;
+constexpr int NSPa = NSP > 0 ? NSP : 1;
+constexpr int NSAa = NSA > 0 ? NSA : 1;
+constexpr int NISAa = NISA > 0 ? NISA : 1;
+constexpr unsigned FULL = 0xffffffffu;
+
+/* shared-memory doubles per warp for U units per lane */
+template <int U>
+struct WarpSmem {
+    static constexpr int NMAX = 32 * U;
+    static constexpr int LDW = NMAX + 1;
+    static constexpr int W_DOUBLES = NMAX * LDW;
+    static constexpr int VEC_DOUBLES = 5 * NMAX;
+    static constexpr int SYS_DOUBLES = NSPa + NSAa + NISAa; /* ints stored in double slots */
+    static constexpr int DOUBLES = W_DOUBLES + VEC_DOUBLES + SYS_DOUBLES;
+    static constexpr int BYTES = DOUBLES * 8;
+};
+
+/* halving-tree sum S(L, i) = S(2L, i) + S(2L, i + L), S(P, i) = leaf(i) */
+template <int L, int P>
+struct TreeSum {
+    template <class Leaf>
+    __device__ __forceinline__ static double run(int i, const Leaf& leaf) {
+        return TreeSum<2 * L, P>::run(i, leaf) + TreeSum<2 * L, P>::run(i + L, leaf);
+    }
+};
+template <int P>
+struct TreeSum<P, P> {
+    template <class Leaf>
+    __device__ __forceinline__ static double run(int i, const Leaf& leaf) { return leaf(i); }
+};
+
+/* Sum over all 32U units of the warp in halving-tree order; every lane gets it. */
+template <int U>
+__device__ __forceinline__ double warp_tree_sum(const double (&v)[U]) {
+    double a[U];
+#pragma unroll
+    for (int m = 0; m < U; m++) a[m] = v[m];
+#pragma unroll
+    for (int h = U / 2; h >= 1; h /= 2)
+#pragma unroll
+        for (int m = 0; m < h; m++) a[m] = a[m] + a[m + h];
+    double s = a[0];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) s = s + __shfl_xor_sync(FULL, s, o);
+    return s;
+}
+
+template <int U>
+__device__ __forceinline__ double warp_tree_max(const double (&v)[U]) {
+    double a[U];
+#pragma unroll
+    for (int m = 0; m < U; m++) a[m] = v[m];
+#pragma unroll
+    for (int h = U / 2; h >= 1; h /= 2)
+#pragma unroll
+        for (int m = 0; m < h; m++) a[m] = fmax(a[m], a[m + h]);
+    double s = a[0];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) s = fmax(s, __shfl_xor_sync(FULL, s, o));
+    return s;
+}
+
+__device__ __forceinline__ double warp_min(double s) {
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) s = fmin(s, __shfl_xor_sync(FULL, s, o));
+    return s;
+}
+
+/* per-warp view of one system */
+template <int U>
+struct Sys {
+    int lane, sid, N;
+    int64_t off, tot;
+    const double* C;
+    double* W;
+    double *vp, *vpt, *vcpt, *vx1, *vxu;
+    double* sPAR;
+    double* sACC;
+    int* isACC;
+    double* gPAR;
+    int* igPAR;
+};
+
+/* A callback may change a system-scope scalar through its reference argument
+ * (the reference's shared variables).  Units see the value from before the
+ * callback round; afterwards the lowest unit that changed it wins. */
+__device__ __forceinline__ double resolve_shared(double before, double after_lane, int first_unit_lane) {
+    unsigned int key = (unsigned int)first_unit_lane;
+    unsigned int best = __reduce_min_sync(FULL, key);
+    if (best == 0xffffffffu) return before;
+    return __shfl_sync(FULL, after_lane, (int)(best & 31u));
+}
+__device__ __forceinline__ int resolve_shared_int(int before, int after_lane, int first_unit_lane) {
+    unsigned int key = (unsigned int)first_unit_lane;
+    unsigned int best = __reduce_min_sync(FULL, key);
+    if (best == 0xffffffffu) return before;
+    return __shfl_sync(FULL, after_lane, (int)(best & 31u));
+}
+
+/* ---------------------------------------------------------------------------
+ * Coupled right-hand side of the whole system (Steppers.cuh:432-562). */
+template <int U>
+__device__ __forceinline__ int coupled_rhs(const Sys<U>& S, const DeviceProblem& P, double T,
+                                           double (&Xs)[U][UD], double (&F)[U][UD],
+                                           double (&up)[U][NUPa], double (&ua)[U][NUAa],
+                                           int (&iua)[U][NIUAa], bool& capped) {
+    constexpr int NMAX = WarpSmem<U>::NMAX;
+    constexpr int LDW = WarpSmem<U>::LDW;
+    const int N = S.N;
+    double xu[U], rd[U], r[U], rt[U], x[U], p[U], pt[U];
+    __syncwarp();
+#pragma unroll
+    for (int m = 0; m < U; m++) {
+        const int i = S.lane + 32 * m;
+        if (i < N) {
+            double Fl[UD], cpt, cpf;
+            CoupledSystems_PerBlock_OdeFunction<double>(S.sid, i, Fl, Xs[m], T, up[m], S.sPAR, S.gPAR, S.igPAR,
+                                                        ua[m], iua[m], S.sACC, S.isACC, &cpt, &cpf);
+#pragma unroll
+            for (int k = 0; k < UD; k++) F[m][k] = Fl[k];
+            xu[m] = Fl[IC];
+            rd[m] = cpf;
+            S.vcpt[i] = cpt;
+            S.vx1[i] = Xs[m][0] * Xs[m][0];
+            S.vxu[i] = Fl[IC];
+        } else {
+#pragma unroll
+            for (int k = 0; k < UD; k++) F[m][k] = 0.0;
+            xu[m] = 0.0;
+            rd[m] = 0.0;
+        }
+    }
+    __syncwarp();
+    /* b = rD (C CPT) + x_u, r = b - A x_u, W_ij = (rD_i C_ij) X1sq_j */
+#pragma unroll
+    for (int m = 0; m < U; m++) {
+        const int i = S.lane + 32 * m;
+        if (i < N) {
+            double b = 0.0, ax = 0.0;
+            const double* Ci = S.C + i;
+            double* Wi = S.W + i;
+#pragma unroll 8
+            for (int j = 0; j < N; j++) {
+                double cij = __ldg(Ci + (int64_t)j * N);
+                double x1 = S.vx1[j];
+                b = fma(cij, S.vcpt[j], b);
+                ax = fma(cij * x1, S.vxu[j], ax);
+                Wi[j * LDW] = (rd[m] * cij) * x1;
+            }
+            b = fma(rd[m], b, xu[m]);
+            ax = fma(rd[m], ax, xu[m]);
+            r[m] = b - ax;
+        } else {
+            r[m] = 0.0;
+        }
+        rt[m] = r[m];
+        x[m] = xu[m];
+        p[m] = 0.0;
+        pt[m] = 0.0;
+    }
+    double prod[U];
+#pragma unroll
+    for (int m = 0; m < U; m++) prod[m] = r[m] * rt[m];
+    double rho1 = warp_tree_sum<U>(prod);
+    double rho2 = 0.0;
+    int done = 0;
+    bool exited = false;
+    for (int iter = 1; iter <= P.bicg_max_iter; iter++) {
+        if (iter == 1) {
+#pragma unroll
+            for (int m = 0; m < U; m++) { p[m] = r[m]; pt[m] = rt[m]; }
+            if (fabs(rho1) < 1e-6) { exited = true; break; }
+        } else {
+            double beta = rho1 / rho2;
+#pragma unroll
+            for (int m = 0; m < U; m++) {
+                p[m] = fma(beta, p[m], r[m]);
+                pt[m] = fma(beta, pt[m], rt[m]);
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int m = 0; m < U; m++) {
+            const int i = S.lane + 32 * m;
+            S.vp[i] = p[m];
+            S.vpt[i] = pt[m];
+        }
+        __syncwarp();
+        double q[U], qt[U];
+#pragma unroll
+        for (int m = 0; m < U; m++) {
+            const int i = S.lane + 32 * m;
+            if (i < N) {
+                double qi = p[m];
+                const double* Wi = S.W + i;
+#pragma unroll 8
+                for (int j = 0; j < N; j++) qi = fma(Wi[j * LDW], S.vp[j], qi);
+                q[m] = qi;
+                const double* Wc = S.W + (int64_t)i * LDW;
+                const double* vpt = S.vpt;
+                auto leaf = [&](int j) -> double { return j < N ? Wc[j] * vpt[j] : 0.0; };
+                qt[m] = pt[m] + TreeSum<1, NMAX>::run(0, leaf);
+            } else {
+                q[m] = 0.0;
+                qt[m] = 0.0;
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < U; m++) prod[m] = pt[m] * q[m];
+        double alpha = rho1 / warp_tree_sum<U>(prod);
+        double ar[U];
+#pragma unroll
+        for (int m = 0; m < U; m++) {
+            x[m] = fma(alpha, p[m], x[m]);
+            r[m] = fma(-alpha, q[m], r[m]);
+            rt[m] = fma(-alpha, qt[m], rt[m]);
+            ar[m] = fabs(r[m]);
+        }
+        double rmax = warp_tree_max<U>(ar);
+        rho2 = rho1;
+        done++;
+        if (rmax < 1e-6) { exited = true; break; }
+#pragma unroll
+        for (int m = 0; m < U; m++) prod[m] = r[m] * rt[m];
+        rho1 = warp_tree_sum<U>(prod);
+    }
+    if (!exited) capped = true;
+#pragma unroll
+    for (int m = 0; m < U; m++) F[m][IC] = x[m];
+    return done;
+}
+
+/* per-lane state of the units it owns */
+template <int U>
+struct Lane {
+    double X[U][UD];
+    double up[U][NUPa];
+    double ua[U][NUAa];
+    int iua[U][NIUAa];
+    double ev_a[U][NEa], ev_n[U][NEa];
+};
+
+struct Counters {
+    unsigned long long acc, rej, bicg, rhs;
+    int status;
+};
+
+template <int U>
+__device__ __forceinline__ bool valid_unit(const Sys<U>& S, int m) { return S.lane + 32 * m < S.N; }
+
+/* ---------------------------------------------------------------------------
+ * RKCK45 step (Steppers.cuh:94-425); returns finiteness of y5 and the error */
+template <int U>
+__device__ __forceinline__ bool step_rkck45(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L,
+                                            double T, double dt, double (&Yn)[U][UD], double (&E)[U][UD],
+                                            Counters& cnt, bool& capped) {
+    double K[6][U][UD];
+    double Xs[U][UD];
+    cnt.bicg += coupled_rhs<U>(S, P, T, L.X, K[0], L.up, L.ua, L.iua, capped);
+#pragma unroll
+    for (int m = 0; m < U; m++)
+#pragma unroll
+        for (int c = 0; c < UD; c++) Xs[m][c] = fma(K[0][m][c] * (1.0 / 5.0), dt, L.X[m][c]);
+    cnt.bicg += coupled_rhs<U>(S, P, fma(1.0 / 5.0, dt, T), Xs, K[1], L.up, L.ua, L.iua, capped);
+#pragma unroll
+    for (int m = 0; m < U; m++)
+#pragma unroll
+        for (int c = 0; c < UD; c++) {
+            double s = K[0][m][c] * (3.0 / 40.0);
+            s = fma(K[1][m][c], 9.0 / 40.0, s);
+            Xs[m][c] = fma(s, dt, L.X[m][c]);
+        }
+    cnt.bicg += coupled_rhs<U>(S, P, fma(3.0 / 10.0, dt, T), Xs, K[2], L.up, L.ua, L.iua, capped);
+#pragma unroll
+    for (int m = 0; m < U; m++)
+#pragma unroll
+        for (int c = 0; c < UD; c++) {
+            double s = K[0][m][c] * (3.0 / 10.0);
+            s = fma(K[1][m][c], -9.0 / 10.0, s);
+            s = fma(K[2][m][c], 6.0 / 5.0, s);
+            Xs[m][c] = fma(s, dt, L.X[m][c]);
+        }
+    cnt.bicg += coupled_rhs<U>(S, P, fma(3.0 / 5.0, dt, T), Xs, K[3], L.up, L.ua, L.iua, capped);
+#pragma unroll
+    for (int m = 0; m < U; m++)
+#pragma unroll
+        for (int c = 0; c < UD; c++) {
+            double s = K[0][m][c] * (-11.0 / 54.0);
+            s = fma(K[1][m][c], 5.0 / 2.0, s);
+            s = fma(K[2][m][c], -70.0 / 27.0, s);
+            s = fma(K[3][m][c], 35.0 / 27.0, s);
+            Xs[m][c] = fma(s, dt, L.X[m][c]);
+        }
+    cnt.bicg += coupled_rhs<U>(S, P, T + dt, Xs, K[4], L.up, L.ua, L.iua, capped);
+#pragma unroll
+    for (int m = 0; m < U; m++)
+#pragma unroll
+        for (int c = 0; c < UD; c++) {
+            double s = K[0][m][c] * (1631.0 / 55296.0);
+            s = fma(K[1][m][c], 175.0 / 512.0, s);
+            s = fma(K[2][m][c], 575.0 / 13824.0, s);
+            s = fma(K[3][m][c], 44275.0 / 110592.0, s);
+            s = fma(K[4][m][c], 253.0 / 4096.0, s);
+            Xs[m][c] = fma(s, dt, L.X[m][c]);
+        }
+    cnt.bicg += coupled_rhs<U>(S, P, fma(7.0 / 8.0, dt, T), Xs, K[5], L.up, L.ua, L.iua, capped);
+    cnt.rhs += 6;
+    bool finite = true;
+#pragma unroll
+    for (int m = 0; m < U; m++)
+#pragma unroll
+        for (int c = 0; c < UD; c++) {
+            double s = K[0][m][c] * (37.0 / 378.0);
+            s = fma(K[2][m][c], 250.0 / 621.0, s);
+            s = fma(K[3][m][c], 125.0 / 594.0, s);
+            s = fma(K[5][m][c], 512.0 / 1771.0, s);
+            Yn[m][c] = fma(s, dt, L.X[m][c]);
+            double e = K[0][m][c] * (37.0 / 378.0 - 2825.0 / 27648.0);
+            e = fma(K[2][m][c], 250.0 / 621.0 - 18575.0 / 48384.0, e);
+            e = fma(K[3][m][c], 125.0 / 594.0 - 13525.0 / 55296.0, e);
+            e = fma(K[4][m][c], 0.0 - 277.0 / 14336.0, e);
+            e = fma(K[5][m][c], 512.0 / 1771.0 - 1.0 / 4.0, e);
+            E[m][c] = fma(dt, fabs(e), 1e-18);
+            if (valid_unit(S, m) && (!isfinite(Yn[m][c]) || !isfinite(E[m][c]))) finite = false;
+        }
+    return __all_sync(FULL, finite);
+}
+
+/* classical RK4 step (the reference has only its fixed-step controller,
+ * ErrorControllers.cuh:424-450) */
+template <int U>
+__device__ __forceinline__ bool step_rk4(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L,
+                                         double T, double dt, double (&Yn)[U][UD], Counters& cnt, bool& capped) {
+    double K[4][U][UD];
+    double Xs[U][UD];
+    cnt.bicg += coupled_rhs<U>(S, P, T, L.X, K[0], L.up, L.ua, L.iua, capped);
+#pragma unroll
+    for (int m = 0; m < U; m++)
+#pragma unroll
+        for (int c = 0; c < UD; c++) Xs[m][c] = fma(K[0][m][c] * 0.5, dt, L.X[m][c]);
+    cnt.bicg += coupled_rhs<U>(S, P, fma(0.5, dt, T), Xs, K[1], L.up, L.ua, L.iua, capped);
+#pragma unroll
+    for (int m = 0; m < U; m++)
+#pragma unroll
+        for (int c = 0; c < UD; c++) Xs[m][c] = fma(K[1][m][c] * 0.5, dt, L.X[m][c]);
+    cnt.bicg += coupled_rhs<U>(S, P, fma(0.5, dt, T), Xs, K[2], L.up, L.ua, L.iua, capped);
+#pragma unroll
+    for (int m = 0; m < U; m++)
+#pragma unroll
+        for (int c = 0; c < UD; c++) Xs[m][c] = fma(K[2][m][c], dt, L.X[m][c]);
+    cnt.bicg += coupled_rhs<U>(S, P, T + dt, Xs, K[3], L.up, L.ua, L.iua, capped);
+    cnt.rhs += 4;
+    bool finite = true;
+#pragma unroll
+    for (int m = 0; m < U; m++)
+#pragma unroll
+        for (int c = 0; c < UD; c++) {
+            double s = K[0][m][c] * (1.0 / 6.0);
+            s = fma(K[1][m][c], 1.0 / 3.0, s);
+            s = fma(K[2][m][c], 1.0 / 3.0, s);
+            s = fma(K[3][m][c], 1.0 / 6.0, s);
+            Yn[m][c] = fma(s, dt, L.X[m][c]);
+            if (valid_unit(S, m) && !isfinite(Yn[m][c])) finite = false;
+        }
+    return __all_sync(FULL, finite);
+}
+
+/* dense-output store (DenseOutput.cuh:312-361), bounds-checked at the slot */
+template <int U>
+__device__ __forceinline__ void store_dense(const Sys<U>& S, const DeviceProblem& P, const Lane<U>& L,
+                                            int& idx, int update_do, int update, int& skipped,
+                                            double& do_time, double T, double TD1) {
+    if (update_do == 1 && idx < P.ndo) {
+#pragma unroll
+        for (int m = 0; m < U; m++) {
+            const int i = S.lane + 32 * m;
+            if (i < S.N) {
+#pragma unroll
+                for (int c = 0; c < UD; c++)
+                    P.dense_state[(int64_t)idx * UD * S.tot + (int64_t)c * S.tot + S.off + i] = L.X[m][c];
+            }
+        }
+        if (S.lane == 0) P.dense_time[(int64_t)idx * P.n_systems + S.sid] = T;
+    }
+    if (update_do == 1) {
+        idx++;
+        skipped = 0;
+        do_time = fmin(T + P.do_min_dt, TD1);
+    }
+    if (update_do == 0 && update == 1) skipped++;
+}
+
+/* ---------------------------------------------------------------------------
+ * One reference Solve() of one system (Solver.cuh:82-648). */
+template <int U>
+__device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, Counters& cnt,
+                           double (&TD)[2], double& T, int& do_idx) {
+    const double TD1 = TD[1];
+    double dt = P.dt0, newdt = P.dt0;
+    int update_do = 1, skipped = 0;
+    double do_time = 0.0;
+    int udt = 0;
+    double rtol[UD], atol[UD];
+#pragma unroll
+    for (int c = 0; c < UD; c++) {
+        rtol[c] = P.rtol[(int64_t)c * P.n_systems + S.sid];
+        atol[c] = P.atol[(int64_t)c * P.n_systems + S.sid];
+    }
+    double evtol[NEa];
+    int evdir[NEa];
+#pragma unroll
+    for (int e = 0; e < NE; e++) { evtol[e] = P.event_tol[e]; evdir[e] = P.event_dir[e]; }
+
+    /* Initialization callback (Solver.cuh:262-280) */
+    {
+        double Tl = T, dTl = dt;
+        int DOl = do_idx;
+        int firstT = -1, firstD = -1, firstO = -1;
+        double TnewL = T, dTnewL = dt;
+        int DOnewL = do_idx;
+#pragma unroll
+        for (int m = 0; m < U; m++) {
+            const int i = S.lane + 32 * m;
+            if (i < S.N) {
+                double Tu = Tl, dTu = dTl;
+                int DOu = DOl;
+                CoupledSystems_PerBlock_Initialization<double>(S.sid, i, DOu, Tu, dTu, TD, L.X[m], L.up[m], S.sPAR,
+                                                               S.gPAR, S.igPAR, L.ua[m], L.iua[m], S.sACC, S.isACC);
+                if (firstT < 0 && Tu != Tl) { firstT = i; TnewL = Tu; }
+                if (firstD < 0 && dTu != dTl) { firstD = i; dTnewL = dTu; }
+                if (firstO < 0 && DOu != DOl) { firstO = i; DOnewL = DOu; }
+            }
+        }
+        T = resolve_shared(T, TnewL, firstT < 0 ? -1 : firstT);
+        dt = resolve_shared(dt, dTnewL, firstD < 0 ? -1 : firstD);
+        newdt = dt;
+        do_idx = resolve_shared_int(do_idx, DOnewL, firstO < 0 ? -1 : firstO);
+    }
+    /* first event values (Solver.cuh:283-305) */
+    if (NE > 0) {
+#pragma unroll
+        for (int m = 0; m < U; m++)
+            if (valid_unit(S, m))
+                CoupledSystems_PerBlock_EventFunction<double>(S.sid, S.lane + 32 * m, L.ev_a[m], T, dt, TD, L.X[m],
+                                                              L.up[m], S.sPAR, S.gPAR, S.igPAR, L.ua[m], L.iua[m],
+                                                              S.sACC, S.isACC);
+    }
+    if (P.ndo > 0) store_dense<U>(S, P, L, do_idx, update_do, 1, skipped, do_time, T, TD1);
+
+    long long attempted = 0;
+    bool terminate = false;
+    while (!terminate) {
+        int update = 1, end = 0;
+        dt = newdt;
+        if (dt > (TD1 - T)) { dt = TD1 - T; end = 1; }
+        if (attempted >= P.max_steps_per_period) { cnt.status |= BES_STATUS_STEP_BUDGET; break; }
+        attempted++;
+        bool capped = false;
+        double Yn[U][UD], E[U][UD];
+        bool finite;
+        if (P.algorithm == 1) {
+            finite = step_rkck45<U>(S, P, L, T, dt, Yn, E, cnt, capped);
+            /* ErrorController_RKCK45 (ErrorControllers.cuh:454-542) */
+            double rr = 1e30;
+            int ru = 1;
+#pragma unroll
+            for (int m = 0; m < U; m++) {
+                if (valid_unit(S, m)) {
+#pragma unroll
+                    for (int c = 0; c < UD; c++) {
+                        double et = fmax(rtol[c] * fmax(fabs(Yn[m][c]), fabs(L.X[m][c])), atol[c]);
+                        ru = ru & (E[m][c] < et);
+                        rr = fmin(rr, et / E[m][c]);
+                    }
+                }
+            }
+            update = __all_sync(FULL, ru) ? 1 : 0;
+            double relerr = warp_min(rr);
+            double mult = update == 1 ? 0.8 * bes::math::pow(relerr, 1.0 / 5.0)
+                                      : 0.8 * bes::math::pow(relerr, 1.0 / 4.0);
+            if (!isfinite(mult)) finite = false;
+            if (!finite) {
+                mult = P.shrink;
+                update = 0;
+                if (dt < P.dtmin * 1.01) { cnt.status |= BES_STATUS_NONFINITE; terminate = true; }
+            } else if (dt < P.dtmin * 1.01) {
+                cnt.status |= BES_STATUS_MIN_STEP;
+                update = 1;
+            }
+            mult = fmin(mult, P.grow);
+            mult = fmax(mult, P.shrink);
+            newdt = dt * mult;
+            newdt = fmin(newdt, P.dtmax);
+            newdt = fmax(newdt, P.dtmin);
+        } else {
+            finite = step_rk4<U>(S, P, L, T, dt, Yn, cnt, capped);
+            if (!finite) { cnt.status |= BES_STATUS_NONFINITE; terminate = true; update = 0; }
+            newdt = P.dt0;
+        }
+        if (__any_sync(FULL, capped)) cnt.status |= BES_STATUS_BICG_CAP;
+
+        if (!terminate && NE > 0) {
+            /* next event values at the trial state (Solver.cuh:393-414) */
+#pragma unroll
+            for (int m = 0; m < U; m++)
+                if (valid_unit(S, m))
+                    CoupledSystems_PerBlock_EventFunction<double>(S.sid, S.lane + 32 * m, L.ev_n[m], T + dt, newdt, TD,
+                                                                  Yn[m], L.up[m], S.sPAR, S.gPAR, S.igPAR, L.ua[m],
+                                                                  L.iua[m], S.sACC, S.isACC);
+            if (update == 1) {
+                /* EventTimeStepControl (EventHandling.cuh:216-268) */
+                double evdt = dt;
+                int corrected = 0;
+#pragma unroll
+                for (int m = 0; m < U; m++) {
+                    if (valid_unit(S, m)) {
+#pragma unroll
+                        for (int e = 0; e < NE; e++) {
+                            double a = L.ev_a[m][e], n = L.ev_n[m][e];
+                            if ((a > evtol[e] && n < -evtol[e] && evdir[e] <= 0) ||
+                                (a < -evtol[e] && n > evtol[e] && evdir[e] >= 0)) {
+                                double cand = (-a) / (n - a) * dt;
+                                evdt = fmin(evdt, cand);
+                                corrected = 1;
+                            }
+                        }
+                    }
+                }
+                if (__any_sync(FULL, corrected)) {
+                    evdt = warp_min(evdt);
+                    if (evdt < P.dtmin) {
+                        cnt.status |= BES_STATUS_EVENT_MISSED;
+                    } else {
+                        newdt = evdt;
+                        update = 0;
+                    }
+                }
+            }
+        }
+
+        if (update == 1) {
+            T = T + dt;
+#pragma unroll
+            for (int m = 0; m < U; m++)
+#pragma unroll
+                for (int c = 0; c < UD; c++) L.X[m][c] = Yn[m][c];
+            cnt.acc++;
+            /* ActionAfterSuccessfulTimeStep (Solver.cuh:443-463) */
+            {
+                double Tl = T, dTl = dt;
+                int firstT = -1, firstD = -1, anyU = 0;
+                double TnewL = T, dTnewL = dt;
+#pragma unroll
+                for (int m = 0; m < U; m++) {
+                    const int i = S.lane + 32 * m;
+                    if (i < S.N) {
+                        double Tu = Tl, dTu = dTl;
+                        int Uu = udt;
+                        CoupledSystems_PerBlock_ActionAfterSuccessfulTimeStep<double>(
+                            S.sid, i, Uu, Tu, dTu, TD, L.X[m], L.up[m], S.sPAR, S.gPAR, S.igPAR, L.ua[m], L.iua[m],
+                            S.sACC, S.isACC);
+                        if (firstT < 0 && Tu != Tl) { firstT = i; TnewL = Tu; }
+                        if (firstD < 0 && dTu != dTl) { firstD = i; dTnewL = dTu; }
+                        if (Uu != udt) anyU = 1;
+                    }
+                }
+                T = resolve_shared(T, TnewL, firstT);
+                dt = resolve_shared(dt, dTnewL, firstD);
+                if (__any_sync(FULL, anyU)) udt = 1;
+            }
+            if (NE > 0) {
+                /* ActionAfterEventDetection when an event lands within tolerance (Solver.cuh:465-495) */
+                double Tl = T, dTl = dt;
+                int firstT = -1, firstD = -1, anyU = 0;
+                double TnewL = T, dTnewL = dt;
+#pragma unroll
+                for (int m = 0; m < U; m++) {
+                    const int i = S.lane + 32 * m;
+                    if (i < S.N) {
+#pragma unroll
+                        for (int e = 0; e < NE; e++) {
+                            double a = L.ev_a[m][e], n = L.ev_n[m][e];
+                            if ((a > evtol[e] && fabs(n) < evtol[e] && evdir[e] <= 0) ||
+                                (a < -evtol[e] && fabs(n) < evtol[e] && evdir[e] >= 0)) {
+                                double Tu = Tl, dTu = dTl;
+                                int Uu = udt;
+                                CoupledSystems_PerBlock_ActionAfterEventDetection<double>(
+                                    S.sid, i, e, Uu, Tu, dTu, TD, L.X[m], L.up[m], S.sPAR, S.gPAR, S.igPAR, L.ua[m],
+                                    L.iua[m], S.sACC, S.isACC);
+                                if (firstT < 0 && Tu != Tl) { firstT = i; TnewL = Tu; }
+                                if (firstD < 0 && dTu != dTl) { firstD = i; dTnewL = dTu; }
+                                if (Uu != udt) anyU = 1;
+                            }
+                        }
+                    }
+                }
+                T = resolve_shared(T, TnewL, firstT);
+                dt = resolve_shared(dt, dTnewL, firstD);
+                if (__any_sync(FULL, anyU)) udt = 1;
+                /* refresh event values at the accepted state (Solver.cuh:497-525) */
+#pragma unroll
+                for (int m = 0; m < U; m++)
+                    if (valid_unit(S, m))
+                        CoupledSystems_PerBlock_EventFunction<double>(S.sid, S.lane + 32 * m, L.ev_a[m], T, newdt, TD,
+                                                                      L.X[m], L.up[m], S.sPAR, S.gPAR, S.igPAR,
+                                                                      L.ua[m], L.iua[m], S.sACC, S.isACC);
+            }
+        } else {
+            cnt.rej++;
+        }
+        if (P.ndo > 0) {
+            /* DenseOutputStorageCondition (DenseOutput.cuh:372-395) */
+            if (update == 1) {
+                update_do = (do_idx < P.ndo && do_time < T && skipped >= (P.do_save_frequency - 1)) ? 1 : 0;
+                if (do_idx < P.ndo && (end == 1 || udt == 1)) update_do = 1;
+            } else {
+                update_do = 0;
+            }
+            store_dense<U>(S, P, L, do_idx, update_do, update, skipped, do_time, T, TD1);
+        }
+        if (update == 1 && (end == 1 || udt == 1)) terminate = true;
+    }
+    /* Finalization callback (Solver.cuh:577-595) */
+    {
+        double Tl = T, dTl = dt;
+        int DOl = do_idx;
+        int firstT = -1, firstD = -1, firstO = -1;
+        double TnewL = T, dTnewL = dt;
+        int DOnewL = do_idx;
+#pragma unroll
+        for (int m = 0; m < U; m++) {
+            const int i = S.lane + 32 * m;
+            if (i < S.N) {
+                double Tu = Tl, dTu = dTl;
+                int DOu = DOl;
+                CoupledSystems_PerBlock_Finalization<double>(S.sid, i, DOu, Tu, dTu, TD, L.X[m], L.up[m], S.sPAR,
+                                                             S.gPAR, S.igPAR, L.ua[m], L.iua[m], S.sACC, S.isACC);
+                if (firstT < 0 && Tu != Tl) { firstT = i; TnewL = Tu; }
+                if (firstD < 0 && dTu != dTl) { firstD = i; dTnewL = dTu; }
+                if (firstO < 0 && DOu != DOl) { firstO = i; DOnewL = DOu; }
+            }
+        }
+        T = resolve_shared(T, TnewL, firstT);
+        do_idx = resolve_shared_int(do_idx, DOnewL, firstO);
+    }
+}
+
+/* ---------------------------------------------------------------------------
+ * The kernel: warps pull systems from the work counter. */
+template <int U>
+__global__ void __launch_bounds__(128) bes_ensemble_kernel(DeviceProblem P) {
+    extern __shared__ double smem[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    double* base = smem + (size_t)wib * WarpSmem<U>::DOUBLES;
+    Sys<U> S;
+    S.lane = lane;
+    S.tot = P.total_units;
+    S.W = base;
+    S.vp = base + WarpSmem<U>::W_DOUBLES;
+    S.vpt = S.vp + WarpSmem<U>::NMAX;
+    S.vcpt = S.vpt + WarpSmem<U>::NMAX;
+    S.vx1 = S.vcpt + WarpSmem<U>::NMAX;
+    S.vxu = S.vx1 + WarpSmem<U>::NMAX;
+    S.sPAR = S.vxu + WarpSmem<U>::NMAX;
+    S.sACC = S.sPAR + NSPa;
+    S.isACC = reinterpret_cast<int*>(S.sACC + NSAa);
+    S.gPAR = P.gpar;
+    S.igPAR = P.igpar;
+
+    Lane<U> L;
+    for (;;) {
+        int k = 0;
+        if (lane == 0) k = atomicAdd(P.work_counter, 1);
+        k = __shfl_sync(FULL, k, 0);
+        if (k >= P.n_active) break;
+        const int sid = P.order ? P.order[k] : k;
+        S.sid = sid;
+        S.N = P.units[sid];
+        S.off = P.unit_offset[sid];
+        S.C = P.coupling + P.coupling_offset[sid];
+        /* unit-scope loads into registers / local memory (Solver.cuh:234-257) */
+#pragma unroll
+        for (int m = 0; m < U; m++) {
+            const int i = lane + 32 * m;
+            const bool v = i < S.N;
+            const int64_t g = S.off + i;
+#pragma unroll
+            for (int c = 0; c < UD; c++) L.X[m][c] = v ? P.state[(int64_t)c * S.tot + g] : 0.0;
+#pragma unroll
+            for (int c = 0; c < NUP; c++) L.up[m][c] = v ? __ldg(P.upar + (int64_t)c * S.tot + g) : 0.0;
+            for (int c = 0; c < NUA; c++) L.ua[m][c] = v ? P.uacc[(int64_t)c * S.tot + g] : 0.0;
+#pragma unroll
+            for (int c = 0; c < NIUA; c++) L.iua[m][c] = v ? P.iuacc[(int64_t)c * S.tot + g] : 0;
+        }
+        /* system-scope loads (Solver.cuh:82-130) */
+        for (int c = lane; c < NSP; c += 32) S.sPAR[c] = P.spar[(int64_t)c * P.n_systems + sid];
+        for (int c = lane; c < NSA; c += 32) S.sACC[c] = P.sacc[(int64_t)c * P.n_systems + sid];
+        for (int c = lane; c < NISA; c += 32) S.isACC[c] = P.isacc[(int64_t)c * P.n_systems + sid];
+        double TD[2] = {P.time_domain[sid], P.time_domain[P.n_systems + sid]};
+        double T = P.actual_time[sid];
+        int do_idx = P.ndo > 0 ? P.dense_index[sid] : 0;
+        __syncwarp();
+        Counters cnt = {0ull, 0ull, 0ull, 0ull, 0};
+        for (int per = 0; per < P.n_periods; per++) {
+            if (per == P.reset_at) {
+#pragma unroll
+                for (int m = 0; m < U; m++) {
+                    for (int c = 0; c < NUA; c++) L.ua[m][c] = lane + 32 * m < S.N ? P.uacc_reset[c] : 0.0;
+#pragma unroll
+                    for (int c = 0; c < NIUA; c++) L.iua[m][c] = lane + 32 * m < S.N ? P.iuacc_reset[c] : 0;
+                }
+            }
+            run_period<U>(S, P, L, cnt, TD, T, do_idx);
+        }
+        /* write-back (Solver.cuh:599-648) */
+        __syncwarp();
+#pragma unroll
+        for (int m = 0; m < U; m++) {
+            const int i = lane + 32 * m;
+            if (i < S.N) {
+                const int64_t g = S.off + i;
+#pragma unroll
+                for (int c = 0; c < UD; c++) P.state[(int64_t)c * S.tot + g] = L.X[m][c];
+                for (int c = 0; c < NUA; c++) P.uacc[(int64_t)c * S.tot + g] = L.ua[m][c];
+#pragma unroll
+                for (int c = 0; c < NIUA; c++) P.iuacc[(int64_t)c * S.tot + g] = L.iua[m][c];
+            }
+        }
+        for (int c = lane; c < NSA; c += 32) P.sacc[(int64_t)c * P.n_systems + sid] = S.sACC[c];
+        for (int c = lane; c < NISA; c += 32) P.isacc[(int64_t)c * P.n_systems + sid] = S.isACC[c];
+        if (lane == 0) {
+            P.actual_time[sid] = T;
+            P.time_domain[sid] = TD[0];
+            P.time_domain[P.n_systems + sid] = TD[1];
+            if (P.ndo > 0) P.dense_index[sid] = do_idx;
+            P.n_accepted[sid] += cnt.acc;
+            P.n_rejected[sid] += cnt.rej;
+            P.n_bicg_iter[sid] += cnt.bicg;
+            P.n_rhs[sid] += cnt.rhs;
+            P.status[sid] |= cnt.status;
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace bes
+
+#endif

@@ -1,0 +1,321 @@
+"""Ensemble builders: Keller-Miksis unit parameters, coupling matrices and the
+benchmark ensembles, as canonical structure-of-arrays inputs.
+
+The parameter formulas restate the reference driver's ``FillSolverObject``
+(CollapseStrength.cu:279-371); the reference coupling format
+``C_ij = CSTR * R_Ej^3 / (R_Ei^2 d_ij)`` (radii and distances in micrometres,
+zero diagonal) is the one of CouplingMatrix_N32_D1_d150_RE2-8.txt, which the
+reference scales by CSTR in ``FillCouplingMatrix`` (CollapseStrength.cu:398-408).
+
+Inputs are synthetic and seeded (numpy PCG64): the reference ships no data set
+beyond its two 32-bubble text files.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Optional
+
+import numpy as np
+
+from . import solver as S
+
+PI = 3.14159265358979323846
+# water at 25 C, exact values of CollapseStrength.cu:291-295
+PV = 3.166775638952003e+03
+RHO = 9.970639504998557e+02
+ST = 0.071977583160056
+VIS = 8.902125058209557e-04
+CL = 1.497251785455527e+03
+P_INF_BAR = 1.0
+KAPPA = 1.4
+NCOLL = 32
+NUP = 21
+NUA = 2 * NCOLL
+
+
+def km_unit_parameters(pa1_bar, f1_khz, pa2_bar, f2_khz, phase, re_um) -> np.ndarray:
+    """The 21 dimensionless unit parameters of CollapseStrength.cu:329-357.
+
+    Arguments broadcast; returns an array of shape (21, ...)."""
+    P1 = np.asarray(pa1_bar, dtype=np.float64)
+    P2 = np.asarray(f1_khz, dtype=np.float64)
+    P3 = np.asarray(pa2_bar, dtype=np.float64)
+    P4 = np.asarray(f2_khz, dtype=np.float64)
+    P5 = np.asarray(phase, dtype=np.float64)
+    P6 = np.asarray(re_um, dtype=np.float64)
+    P1, P2, P3, P4, P5, P6 = np.broadcast_arrays(P1, P2, P3, P4, P5, P6)
+    P7, P9 = P_INF_BAR, KAPPA
+    Pinf = P7 * 1e5
+    PA1 = P1 * 1e5
+    PA2 = P3 * 1e5
+    RE = P6 / 1e6
+    f1 = 2.0 * PI * (P2 * 1000)
+    f2 = 2.0 * PI * (P4 * 1000)
+    w = (2.0 * PI / RE / f1) ** 2.0
+    u = np.empty((NUP,) + P1.shape, dtype=np.float64)
+    u[0] = (2.0 * ST / RE + Pinf - PV) * w / RHO
+    u[1] = (1.0 - 3.0 * P9) * (2 * ST / RE + Pinf - PV) * (2.0 * PI / RE / f1) / CL / RHO
+    u[2] = (Pinf - PV) * w / RHO
+    u[3] = (2.0 * ST / RE / RHO) * w
+    u[4] = (4.0 * VIS / RHO / RE ** 2.0) * (2.0 * PI / f1)
+    u[5] = PA1 * w / RHO
+    u[6] = PA2 * w / RHO
+    u[7] = (RE * f1 * PA1 / RHO / CL) * w
+    u[8] = (RE * f2 * PA2 / RHO / CL) * w
+    u[9] = RE * f1 / (2.0 * PI) / CL
+    u[10] = 3.0 * P9
+    with np.errstate(divide="ignore", invalid="ignore"):
+        u[11] = np.where(P2 != 0, P4 / P2, 0.0)
+    u[12] = P5
+    u[13] = 2.0 * PI / f1
+    u[14] = RE
+    u[15] = P1
+    u[16] = P2
+    u[17] = P3
+    u[18] = P4
+    u[19] = P5
+    u[20] = P6
+    return u
+
+
+def coupling_from_geometry(positions_um: np.ndarray, radii_um: np.ndarray, cstr: float = 1.0) -> np.ndarray:
+    """Reference-format coupling matrix C[i, j] = cstr R_j^3 / (R_i^2 d_ij), C[i, i] = 0."""
+    x = np.asarray(positions_um, dtype=np.float64)
+    if x.ndim == 1:
+        x = x[:, None]
+    r = np.asarray(radii_um, dtype=np.float64)
+    d = np.sqrt(((x[:, None, :] - x[None, :, :]) ** 2).sum(-1))
+    n = len(r)
+    C = np.zeros((n, n))
+    off = ~np.eye(n, dtype=bool)
+    C[off] = (cstr * (r[None, :] ** 3) / (r[:, None] ** 2 * np.where(off, d, 1.0)))[off]
+    return C
+
+
+def linspace_ref(b: float, e: float, n: int) -> np.ndarray:
+    """Linspace of CollapseStrength.cu:208-224 (end points exact)."""
+    x = np.empty(n)
+    x[0] = b
+    if n > 1:
+        x[n - 1] = e
+        inc = (e - b) / (n - 1)
+        for i in range(1, n - 1):
+            x[i] = b + i * inc
+    return x
+
+
+def logspace_ref(b: float, e: float, n: int) -> np.ndarray:
+    """Logspace of CollapseStrength.cu:226-241 (end points exact)."""
+    x = np.empty(n)
+    x[0] = b
+    if n > 1:
+        x[n - 1] = e
+        eb, ee = math.log10(b), math.log10(e)
+        inc = (ee - eb) / (n - 1)
+        for i in range(1, n - 1):
+            x[i] = 10.0 ** (eb + i * inc)
+    return x
+
+
+@dataclasses.dataclass
+class Ensemble:
+    """A whole ensemble in the library's canonical layout."""
+    units: np.ndarray                 # [NS] int32
+    upar: np.ndarray                  # [NUP, TU]
+    state: np.ndarray                 # [2, TU]
+    coupling: np.ndarray              # matrices back to back, column-major
+    matrix_of_system: np.ndarray      # [NS] int32
+    rtol: np.ndarray                  # [2, NS]
+    atol: np.ndarray                  # [2, NS]
+    dt0: float = 1e-3
+    dtmin: float = 1e-13
+    dtmax: float = 1e6
+    grow: float = 5.0
+    shrink: float = 0.1
+    event_tol: float = 1e-4
+    event_dir: int = -1
+    n_periods: int = 64
+    reset_at: int = 32
+    max_steps_per_period: int = 1_000_000
+    name: str = ""
+    info: dict = dataclasses.field(default_factory=dict)
+
+    @property
+    def n_systems(self) -> int:
+        return int(len(self.units))
+
+    @property
+    def total_units(self) -> int:
+        return int(self.units.sum())
+
+    @property
+    def unit_offset(self) -> np.ndarray:
+        return np.concatenate([[0], np.cumsum(self.units)[:-1]]).astype(np.int64)
+
+    @property
+    def n_matrices(self) -> int:
+        return int(self.matrix_of_system.max()) + 1
+
+    def matrix_offsets(self) -> np.ndarray:
+        dims = np.zeros(self.n_matrices, dtype=np.int64)
+        dims[self.matrix_of_system] = self.units
+        return np.concatenate([[0], np.cumsum(dims * dims)[:-1]]).astype(np.int64)
+
+    def coupling_offset(self) -> np.ndarray:
+        return self.matrix_offsets()[self.matrix_of_system]
+
+    def initial_uacc(self) -> np.ndarray:
+        return np.zeros((NUA, self.total_units))
+
+    def initial_iuacc(self) -> np.ndarray:
+        return np.full((1, self.total_units), -1, dtype=np.int32)
+
+    def subset(self, systems) -> "Ensemble":
+        """The ensemble restricted to the listed systems (each keeps its own matrix)."""
+        systems = np.asarray(systems, dtype=np.int64)
+        off = self.unit_offset
+        cols = np.concatenate([np.arange(off[s], off[s] + self.units[s]) for s in systems])
+        moff = self.matrix_offsets()
+        mats, new_mos, blocks = {}, [], []
+        for s in systems:
+            m = int(self.matrix_of_system[s])
+            if m not in mats:
+                n = int(self.units[s])
+                mats[m] = len(mats)
+                blocks.append(self.coupling[moff[m]:moff[m] + n * n])
+            new_mos.append(mats[m])
+        return dataclasses.replace(
+            self, units=self.units[systems].copy(), upar=self.upar[:, cols].copy(), state=self.state[:, cols].copy(),
+            coupling=np.concatenate(blocks), matrix_of_system=np.asarray(new_mos, dtype=np.int32),
+            rtol=self.rtol[:, systems].copy(), atol=self.atol[:, systems].copy(), info=dict(self.info))
+
+    def make_solver(self, device: int = 0, **kw) -> S.ProblemSolver:
+        """Create a ProblemSolver filled with this ensemble (host mirrors only; call H2D)."""
+        ps = S.ProblemSolver(self.n_systems, self.units if len(set(self.units.tolist())) > 1 else int(self.units[0]),
+                             n_coupling_matrices=self.n_matrices, coupling_matrix_of_system=self.matrix_of_system,
+                             device=device, **kw)
+        self.fill(ps)
+        return ps
+
+    def fill(self, ps: S.ProblemSolver) -> None:
+        V, O = S.ListOfVariables, S.ListOfSolverOptions
+        ps.set_array(V.ActualState, self.state)
+        ps.set_array(V.UnitParameters, self.upar)
+        ps.set_array(V.UnitAccessories, self.initial_uacc())
+        ps.set_array(V.IntegerUnitAccessories, self.initial_iuacc())
+        td = np.zeros((2, self.n_systems))
+        td[1] = 1.0
+        ps.set_array(V.TimeDomain, td)
+        ps.set_array(V.ActualTime, np.zeros(self.n_systems))
+        ps.set_array(V.CouplingMatrix, self.coupling)
+        ps.set_array(V.CouplingStrength, np.ones(self.n_systems))
+        ps.set_array(V.CouplingIndex, np.ones(1, dtype=np.int32))
+        ps.set_array(V.RelativeToleranceSystem, self.rtol)
+        ps.set_array(V.AbsoluteToleranceSystem, self.atol)
+        ps.SolverOption(O.InitialTimeStep, self.dt0)
+        ps.SolverOption(O.MinimumTimeStep, self.dtmin)
+        ps.SolverOption(O.MaximumTimeStep, self.dtmax)
+        ps.SolverOption(O.TimeStepGrowLimit, self.grow)
+        ps.SolverOption(O.TimeStepShrinkLimit, self.shrink)
+        ps.SolverOption(O.EventTolerance, 0, self.event_tol)
+        ps.SolverOption(O.EventDirection, 0, self.event_dir)
+        ps.SolverOption(O.MaxStepsPerPeriod, self.max_steps_per_period)
+        ps.set_accessory_reset(np.zeros(NUA), np.array([-1], dtype=np.int32))
+
+
+def c1_ensemble(n_pa: int = 16, n_f: int = 16, n_units: int = 32, spacing_um: float = 150.0,
+                seed: int = 1, rtol: float = 1e-10, atol: float = 1e-10, n_periods: int = 64,
+                reset_at: int = 32, cstr: float = 1.0, pa_range=(0.5, 2.0), f_range=(20.0, 200.0)) -> Ensemble:
+    """Plain-method small ensemble: n_pa x n_f systems of N bubbles on a 1-D line.
+
+    Amplitude linspace over pa_range (bar), frequency logspace over f_range
+    (kHz), frequency outer and amplitude inner as in CollapseStrength.cu:306-308;
+    equilibrium radii U(2, 8) um from PCG64(seed), bubble i at x = spacing * i."""
+    rng = np.random.default_rng(seed)
+    radii = rng.uniform(2.0, 8.0, n_units)
+    pos = spacing_um * np.arange(n_units, dtype=np.float64)
+    C = coupling_from_geometry(pos, radii, cstr)
+    pa = linspace_ref(pa_range[0], pa_range[1], n_pa)
+    fr = logspace_ref(f_range[0], f_range[1], n_f)
+    ns = n_pa * n_f
+    sys_pa = np.tile(pa, n_f)
+    sys_f = np.repeat(fr, n_pa)
+    up = km_unit_parameters(sys_pa[:, None], sys_f[:, None], 0.0, 0.0, 0.0, radii[None, :])  # [21, NS, N]
+    upar = up.reshape(NUP, ns * n_units)
+    state = np.zeros((2, ns * n_units))
+    state[0] = 1.0
+    return Ensemble(units=np.full(ns, n_units, dtype=np.int32), upar=upar, state=state,
+                    coupling=C.T.reshape(-1).copy(), matrix_of_system=np.zeros(ns, dtype=np.int32),
+                    rtol=np.full((2, ns), rtol), atol=np.full((2, ns), atol), n_periods=n_periods, reset_at=reset_at,
+                    name=f"c1_{ns}x{n_units}", info={"pa_bar": sys_pa, "f_khz": sys_f, "radii_um": radii,
+                                                     "positions_um": pos, "cstr": cstr})
+
+
+def c2_ensemble(n_systems: int = 16384, seed: int = 2, n_periods: int = 64, reset_at: int = 32,
+                sizes=(4, 8, 16, 32, 48, 64), sphere_um: float = 500.0, min_sep_um: float = 20.0) -> Ensemble:
+    """Uneven ensemble: N from `sizes`, random 3-D clouds in a sphere with a
+    minimum separation, radii U(1, 10) um, dual-frequency drive f2 = k f1
+    (k in {2, 3}), amplitudes U(0, 1.5) bar, tolerances 1e-8 / 1e-10 alternating."""
+    rng = np.random.default_rng(seed)
+    units = rng.choice(np.asarray(sizes), n_systems).astype(np.int32)
+    ups, coups, states = [], [], []
+    rtol = np.empty((2, n_systems))
+    for s in range(n_systems):
+        n = int(units[s])
+        pts = []
+        while len(pts) < n:
+            p = rng.uniform(-sphere_um, sphere_um, 3)
+            if p @ p > sphere_um ** 2:
+                continue
+            if all(np.linalg.norm(p - q) >= min_sep_um for q in pts):
+                pts.append(p)
+        pts = np.asarray(pts)
+        r = rng.uniform(1.0, 10.0, n)
+        f1 = rng.uniform(20.0, 100.0)
+        k = int(rng.integers(2, 4))
+        pa1, pa2 = rng.uniform(0.0, 1.5, 2)
+        ups.append(km_unit_parameters(pa1, f1, pa2, k * f1, 0.0, r))
+        coups.append(coupling_from_geometry(pts, r).T.reshape(-1))
+        st = np.zeros((2, n))
+        st[0] = 1.0
+        states.append(st)
+        rtol[:, s] = 1e-8 if s % 2 == 0 else 1e-10
+    return Ensemble(units=units, upar=np.concatenate(ups, axis=1), state=np.concatenate(states, axis=1),
+                    coupling=np.concatenate(coups), matrix_of_system=np.arange(n_systems, dtype=np.int32),
+                    rtol=rtol, atol=rtol.copy(), n_periods=n_periods, reset_at=reset_at,
+                    name=f"c2_{n_systems}_mixed")
+
+
+def c3_ensemble(n_systems: int = 4096, n_units: int = 128, seed: int = 3, n_periods: int = 4, reset_at: int = -1,
+                cube_um: float = 1000.0, pa_bar: float = 1.2, f_khz: float = 200.0, rtol: float = 1e-10,
+                perturbation: float = 1e-3) -> Ensemble:
+    """Shared-geometry ensemble: one N-bubble cloud (uniform in a cube, radii
+    lognormal median 4 um, sigma 0.4, clipped to [1, 12] um) shared by every
+    system; systems differ by a perturbed initial radius
+    y1(0) = 1 + perturbation * U(-1, 1) per bubble."""
+    rng = np.random.default_rng(seed)
+    pts = rng.uniform(0.0, cube_um, (n_units, 3))
+    r = np.clip(np.exp(np.log(4.0) + 0.4 * rng.standard_normal(n_units)), 1.0, 12.0)
+    C = coupling_from_geometry(pts, r)
+    up = km_unit_parameters(pa_bar, f_khz, 0.0, 0.0, 0.0, r)
+    upar = np.tile(up, (1, n_systems))
+    state = np.zeros((2, n_systems * n_units))
+    state[0] = 1.0 + perturbation * rng.uniform(-1.0, 1.0, n_systems * n_units)
+    return Ensemble(units=np.full(n_systems, n_units, dtype=np.int32), upar=upar, state=state,
+                    coupling=C.T.reshape(-1).copy(), matrix_of_system=np.zeros(n_systems, dtype=np.int32),
+                    rtol=np.full((2, n_systems), rtol), atol=np.full((2, n_systems), rtol), n_periods=n_periods,
+                    reset_at=reset_at, name=f"c3_{n_systems}x{n_units}_shared")
+
+
+def collapse_records(uacc: np.ndarray, iuacc: np.ndarray, units: np.ndarray):
+    """Per-unit (Rmax_k, Rmin_k, Rmax_k/Rmin_k) for the recorded collapses and the event count.
+
+    uacc [64, TU], iuacc [1, TU]: slots 0..31 hold radius maxima (R/R_E),
+    slots 32..63 the minima that follow them (BubbleEnsemble_SystemDefinition.cuh:79-105)."""
+    count = iuacc[0].astype(np.int64) + 1
+    rmax = uacc[:NCOLL]
+    rmin = uacc[NCOLL:2 * NCOLL]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        strength = np.where(rmin > 0, rmax / rmin, 0.0)
+    return rmax, rmin, strength, count

@@ -1,0 +1,245 @@
+/*
+ * bes.h -- C ABI of the B200 ensemble integrator for coupled Keller-Miksis
+ * bubble systems ("bes" = bubble ensemble solver).
+ *
+ * This is the drop-in boundary for the reference's host API, the compile-time
+ * C++ class ProblemSolver<NS,UPS,UD,TPB,SPB,NC,CBW,CCI,NUP,NSP,NGP,NiGP,NUA,
+ * NiUA,NSA,NiSA,NE,NDO,Algorithm,Precision>
+ * (SourceCodes/CoupledSystems_PerBlock_Interface.cuh:135-248).  Each entry
+ * point below names the member function it replaces.  Plain C types only: a
+ * ctypes / cgo / JNI binding needs nothing else.  include/bes_problem_solver.h
+ * rebuilds the reference's template class on top of these calls.
+ *
+ * Differences from the reference, by design:
+ *   - sizes are run-time values (bes_config) and unit counts may differ per
+ *     system; the system definition (the seven device callbacks and their
+ *     sizes) is compiled into the library, and bes_create checks the sizes;
+ *   - every call returns a bes_status instead of calling exit() (the
+ *     reference exits on bad indices, Interface.cuh:718-733, and on CUDA
+ *     errors, :13-22); bes_last_error() gives the message;
+ *   - bes_solve_periods() runs many Solve() periods, with the accessory reset
+ *     between the transient and the recorded phase, in one kernel launch;
+ *   - per-system status and counters (steps, rejections, BiCG iterations)
+ *     are returned to the host.
+ * A handle is not thread-safe; separate handles are independent.
+ */
+#ifndef BES_H
+#define BES_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t bes_status;
+#define BES_OK 0
+#define BES_ERR_ARGUMENT 1      /* null pointer, bad size or value */
+#define BES_ERR_INDEX 2         /* index out of range (reference: BoundCheck, Interface.cuh:718-733) */
+#define BES_ERR_OPTION 3        /* option/variable not valid for this call (reference: exit in the switch defaults) */
+#define BES_ERR_CUDA 4          /* CUDA runtime error (reference: gpuErrCHK, Interface.cuh:13-22) */
+#define BES_ERR_MEMORY 5        /* allocation failed or too large (reference: Interface.cuh:463-471) */
+#define BES_ERR_IO 6            /* input file missing or malformed */
+#define BES_ERR_MODEL 7         /* sizes do not match the compiled system definition */
+#define BES_ERR_UNSUPPORTED 8   /* feature outside this build (e.g. banded coupling storage) */
+
+/* ListOfVariables, same names and order as Interface.cuh:35-53 */
+#define BES_ALL 0
+#define BES_TIME_DOMAIN 1
+#define BES_ACTUAL_TIME 2
+#define BES_ACTUAL_STATE 3
+#define BES_UNIT_PARAMETERS 4
+#define BES_SYSTEM_PARAMETERS 5
+#define BES_GLOBAL_PARAMETERS 6
+#define BES_INTEGER_GLOBAL_PARAMETERS 7
+#define BES_UNIT_ACCESSORIES 8
+#define BES_INTEGER_UNIT_ACCESSORIES 9
+#define BES_SYSTEM_ACCESSORIES 10
+#define BES_INTEGER_SYSTEM_ACCESSORIES 11
+#define BES_COUPLING_MATRIX 12
+#define BES_COUPLING_STRENGTH 13
+#define BES_COUPLING_INDEX 14
+#define BES_DENSE_OUTPUT 15
+#define BES_DENSE_INDEX 16
+#define BES_DENSE_TIME 17
+#define BES_DENSE_STATE 18
+/* extensions (no reference counterpart) */
+#define BES_RELATIVE_TOLERANCE_SYSTEM 100  /* [UD][n_systems] per-system relative tolerances */
+#define BES_ABSOLUTE_TOLERANCE_SYSTEM 101  /* [UD][n_systems] per-system absolute tolerances */
+#define BES_COUNTERS 102                   /* per-system counters and status (device -> host only) */
+
+/* ListOfSolverOptions, same names and order as Interface.cuh:55-68 */
+#define BES_OPT_INITIAL_TIME_STEP 0
+#define BES_OPT_ACTIVE_SYSTEMS 1
+#define BES_OPT_MAXIMUM_TIME_STEP 2
+#define BES_OPT_MINIMUM_TIME_STEP 3
+#define BES_OPT_TIME_STEP_GROW_LIMIT 4
+#define BES_OPT_TIME_STEP_SHRINK_LIMIT 5
+#define BES_OPT_RELATIVE_TOLERANCE 6
+#define BES_OPT_ABSOLUTE_TOLERANCE 7
+#define BES_OPT_EVENT_TOLERANCE 8
+#define BES_OPT_EVENT_DIRECTION 9
+#define BES_OPT_DENSE_OUTPUT_SAVE_FREQUENCY 10
+#define BES_OPT_DENSE_OUTPUT_MINIMUM_TIME_STEP 11
+#define BES_OPT_SHARED_GLOBAL_VARIABLES 12
+#define BES_OPT_SHARED_COUPLING_MATRICES 13
+/* extensions */
+#define BES_OPT_MAX_STEPS_PER_PERIOD 100   /* attempted steps per period before BES_STATUS_STEP_BUDGET (default 1e6) */
+#define BES_OPT_BICG_MAX_ITERATIONS 101    /* the reference's loop runs 19 iterations (Steppers.cuh:508) */
+#define BES_OPT_WARPS_PER_BLOCK 102        /* launch shape: systems (warps) per CTA, 0 = automatic */
+
+/* Algorithms, Interface.cuh:33 */
+#define BES_RK4 0
+#define BES_RKCK45 1
+
+/* per-system status bits (the reference only printf()s these) */
+#define BES_STATUS_NONFINITE 1
+#define BES_STATUS_MIN_STEP 2
+#define BES_STATUS_STEP_BUDGET 4
+#define BES_STATUS_EVENT_MISSED 8
+#define BES_STATUS_BICG_CAP 16
+
+typedef struct bes_solver bes_solver;
+
+/* Problem sizes: the reference's template parameters
+ * (CollapseStrength.cu:34-54), as run-time values. */
+typedef struct bes_config {
+    int32_t device;
+    int32_t n_systems;                 /* NS */
+    int32_t units_per_system;          /* UPS for uniform ensembles; 0 when `units` is given */
+    const int32_t* units;              /* optional [n_systems] unit count per system (1..128) */
+    int32_t unit_dim;                  /* UD */
+    int32_t n_unit_parameters;         /* NUP */
+    int32_t n_system_parameters;       /* NSP */
+    int32_t n_global_parameters;       /* NGP */
+    int32_t n_int_global_parameters;   /* NiGP */
+    int32_t n_unit_accessories;        /* NUA */
+    int32_t n_int_unit_accessories;    /* NiUA */
+    int32_t n_system_accessories;      /* NSA */
+    int32_t n_int_system_accessories;  /* NiSA */
+    int32_t n_events;                  /* NE */
+    int32_t n_dense_output;            /* NDO */
+    int32_t n_couplings;               /* NC; coupling 0 enters the implicit solve (as in the reference) */
+    int32_t coupling_bandwidth;        /* CBW; must be 0 (full storage) */
+    int32_t coupling_circular;         /* CCI; must be 0 */
+    int32_t algorithm;                 /* BES_RK4 or BES_RKCK45 */
+    int32_t n_coupling_matrices;       /* distinct geometries; 1 = one matrix for every system (the reference) */
+    const int32_t* coupling_matrix_of_system; /* optional [n_systems]; default s -> 0, or s -> s when
+                                                 n_coupling_matrices == n_systems */
+} bes_config;
+
+/* sizes of the system definition compiled into the library */
+typedef struct bes_model_info {
+    int32_t unit_dim, n_unit_parameters, n_system_parameters, n_global_parameters, n_int_global_parameters;
+    int32_t n_unit_accessories, n_int_unit_accessories, n_system_accessories, n_int_system_accessories;
+    int32_t n_events;
+    int32_t max_units_per_system;
+    char name[64];
+} bes_model_info;
+
+typedef struct bes_counters {
+    uint64_t accepted_steps;
+    uint64_t rejected_steps;
+    uint64_t bicg_iterations;          /* completed BiCG iterations summed over all right-hand sides */
+    uint64_t rhs_evaluations;
+    int32_t status;                    /* OR of BES_STATUS_* */
+    int32_t units;
+} bes_counters;
+
+/* ProblemSolver::ProblemSolver(int Device), Interface.cuh:354-657: allocates
+ * pinned host mirrors and device arrays, sets the default options
+ * (Interface.cuh:613-635). */
+bes_status bes_create(const bes_config* config, bes_solver** out);
+/* ProblemSolver::~ProblemSolver, Interface.cuh:661-714 */
+bes_status bes_destroy(bes_solver* h);
+/* sizes of the compiled system definition (BubbleEnsemble_SystemDefinition.cuh) */
+bes_status bes_model_info_get(bes_model_info* out);
+
+/* ProblemSolver::SolverOption(ListOfSolverOptions, T), Interface.cuh:774-827 */
+bes_status bes_solver_option(bes_solver* h, int32_t option, double value);
+/* ProblemSolver::SolverOption(ListOfSolverOptions, int, T), Interface.cuh:832-865 */
+bes_status bes_solver_option_indexed(bes_solver* h, int32_t option, int32_t index, double value);
+
+/* ProblemSolver::SetHost overloads (SourceCodes/CoupledSystems_PerBlock_Interface.cuh):
+ * unit scope :870-910, system scope and dense time :914-965, global scope :969-997,
+ * coupling matrix :1001-1087, dense index :1091-1110, dense state :1114-1140.
+ * With several coupling matrices, `n` = matrix * n_couplings + coupling. */
+bes_status bes_set_host_unit(bes_solver* h, int32_t sid, int32_t uid, int32_t var, int32_t k, double value);
+bes_status bes_set_host_system(bes_solver* h, int32_t sid, int32_t var, int32_t k, double value);
+bes_status bes_set_host_global(bes_solver* h, int32_t var, int32_t k, double value);
+bes_status bes_set_host_coupling(bes_solver* h, int32_t n, int32_t var, int32_t row, int32_t col, double value);
+bes_status bes_set_host_dense_index(bes_solver* h, int32_t sid, int32_t var, double value);
+bes_status bes_set_host_dense_state(bes_solver* h, int32_t sid, int32_t uid, int32_t var, int32_t comp,
+                                    int32_t slot, double value);
+/* ProblemSolver::GetHost overloads: unit :1341-1377, system and dense time :1381-1425,
+ * global :1429-1454, coupling matrix :1458-1478, dense index :1482-1500, dense state :1504-1529 */
+bes_status bes_get_host_unit(bes_solver* h, int32_t sid, int32_t uid, int32_t var, int32_t k, double* value);
+bes_status bes_get_host_system(bes_solver* h, int32_t sid, int32_t var, int32_t k, double* value);
+bes_status bes_get_host_global(bes_solver* h, int32_t var, int32_t k, double* value);
+bes_status bes_get_host_coupling(bes_solver* h, int32_t n, int32_t var, int32_t row, int32_t col, double* value);
+bes_status bes_get_host_dense_index(bes_solver* h, int32_t sid, int32_t var, double* value);
+bes_status bes_get_host_dense_state(bes_solver* h, int32_t sid, int32_t uid, int32_t var, int32_t comp,
+                                    int32_t slot, double* value);
+
+/* Bulk copy between a caller array and the host mirror, in the canonical
+ * layout (unit scope [k][total_units], system scope [k][n_systems], coupling
+ * matrices back to back, column-major).  `count` is in elements; integer
+ * variables take int32_t, the rest double.  No reference counterpart (the
+ * reference only has element-wise SetHost/GetHost). */
+bes_status bes_set_array(bes_solver* h, int32_t var, const void* src, int64_t count);
+bes_status bes_get_array(bes_solver* h, int32_t var, void* dst, int64_t count);
+bes_status bes_array_size(bes_solver* h, int32_t var, int64_t* count);
+
+/* ProblemSolver::SynchroniseFromHostToDevice, Interface.cuh:1144-1238, and
+ * SynchroniseFromDeviceToHost, Interface.cuh:1242-1336
+ * (asynchronous on the solver's stream, like the reference) */
+bes_status bes_synchronise_host_to_device(bes_solver* h, int32_t var);
+bes_status bes_synchronise_device_to_host(bes_solver* h, int32_t var);
+
+/* ProblemSolver::Solve, Interface.cuh:1951-1956: one period (one kernel launch),
+ * asynchronous. */
+bes_status bes_solve(bes_solver* h);
+/* The driver loop of CollapseStrength.cu:123-147 (n Solve() calls, accessories
+ * reset before period `reset_at`, -1 for never) in one persistent launch. */
+bes_status bes_solve_periods(bes_solver* h, int32_t n_periods, int32_t reset_at);
+/* reset values for bes_solve_periods (CollapseStrength.cu:373-396 resets every
+ * unit's accessories to 0 and its integer accessory to -1) */
+bes_status bes_set_accessory_reset(bes_solver* h, const double* uacc, const int32_t* iuacc);
+
+/* ProblemSolver::SynchroniseDevice / InsertSynchronisationPoint / SynchroniseSolver,
+ * Interface.cuh:1960-1983 */
+bes_status bes_synchronise_device(bes_solver* h);
+bes_status bes_insert_synchronisation_point(bes_solver* h);
+bes_status bes_synchronise_solver(bes_solver* h);
+
+/* Use the caller's CUDA stream (a cudaStream_t) instead of the solver's own. */
+bes_status bes_set_stream(bes_solver* h, void* cuda_stream);
+/* device time of the last bes_solve / bes_solve_periods, measured with CUDA
+ * events around its launches (valid after bes_synchronise_solver) */
+bes_status bes_last_solve_ms(bes_solver* h, float* ms);
+/* number of kernel launches the last bes_solve / bes_solve_periods issued */
+bes_status bes_last_solve_launches(bes_solver* h, int32_t* launches);
+
+/* per-system counters from the host mirror; call
+ * bes_synchronise_device_to_host(h, BES_COUNTERS) and sync first */
+bes_status bes_get_counters(bes_solver* h, int32_t sid, bes_counters* out);
+/* zero the device counters and status words */
+bes_status bes_reset_counters(bes_solver* h);
+
+/* LoadBubbleSizes, CollapseStrength.cu:245-258: n whitespace-separated numbers */
+bes_status bes_load_bubble_sizes(const char* path, int32_t n, double* out);
+/* LoadCouplingMatrix, CollapseStrength.cu:260-277: n x n numbers, row by row,
+ * written to out[row * n + col] */
+bes_status bes_load_coupling_matrix(const char* path, int32_t n, double* out);
+
+/* ListCUDADevices, Interface.cuh:260-311 */
+bes_status bes_device_count(int32_t* count);
+
+const char* bes_status_string(bes_status status);
+const char* bes_last_error(const bes_solver* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

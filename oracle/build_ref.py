@@ -1,0 +1,74 @@
+"""TEST INFRASTRUCTURE: build recipe for the reference's own CUDA solver.
+
+Compiles oracle/ref_harness.cu against the reference's unmodified headers in
+place (``/root/reference`` and ``/root/reference/SourceCodes``) with the
+reference's own nvcc flags (makefile:2), except ``sm_100a`` for ``sm_35``.
+Outputs go to ``oracle/_ref/`` only (git-ignored; the built binaries travel
+with the tree to the GPU machine, the reference sources do not).
+
+Variants: ``ref_n{UPS}_s{NS}_d{NDO}`` with the shipped ``-maxrregcount=128``
+and ``..._nocap`` without it.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+OUT = HERE / "_ref"
+REFERENCE = Path(os.environ.get("BES_REFERENCE_DIR", "/root/reference"))
+
+# (units per system, max systems, dense-output slots, register cap)
+VARIANTS = [
+    (32, 256, 0, True), (32, 256, 0, False),
+    (32, 64, 16, True),
+    (64, 64, 0, True),
+    (128, 16, 0, True),
+]
+
+
+def name(ups: int, ns: int, ndo: int, cap: bool) -> str:
+    return f"ref_n{ups}_s{ns}_d{ndo}" + ("" if cap else "_nocap")
+
+
+def path(ups: int, ns: int, ndo: int = 0, cap: bool = True) -> Path:
+    return OUT / name(ups, ns, ndo, cap)
+
+
+def available() -> bool:
+    return (REFERENCE / "SourceCodes" / "CoupledSystems_PerBlock_Interface.cuh").exists()
+
+
+def _one(v) -> Path:
+    ups, ns, ndo, cap = v
+    exe = path(ups, ns, ndo, cap)
+    src = HERE / "ref_harness.cu"
+    if exe.exists() and exe.stat().st_mtime > src.stat().st_mtime:
+        return exe
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    cmd = [nvcc, "-O3", "--std=c++11", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-w",
+           f"-DHARNESS_UPS={ups}", f"-DHARNESS_NS={ns}", f"-DHARNESS_NDO={ndo}",
+           "-I", str(REFERENCE), "-I", str(REFERENCE / "SourceCodes"), str(src), "-o", str(exe)]
+    if cap:
+        cmd.insert(1, "-maxrregcount=128")
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"reference build failed ({exe.name}):\n{res.stderr[-4000:]}")
+    return exe
+
+
+def build() -> list[Path]:
+    """Build every variant (no-op when the reference tree is absent)."""
+    if not available():
+        return []
+    OUT.mkdir(exist_ok=True)
+    with cf.ThreadPoolExecutor(max_workers=min(len(VARIANTS), os.cpu_count() or 1)) as ex:
+        return list(ex.map(_one, VARIANTS))
+
+
+if __name__ == "__main__":
+    for p in build():
+        print(p)

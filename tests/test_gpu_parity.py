@@ -1,0 +1,74 @@
+"""Parity of the sm_100a kernel with the CPU oracle (bit for bit).
+
+Kernel and oracle follow the same arithmetic order with explicit fused
+multiply-adds and the same elementary functions, so every output must be
+identical: states, collapse records, event counts, step/BiCG counters,
+status bits and dense output."""
+import numpy as np
+import pytest
+
+from bubbleensemble_implicitextension_b200 import solver as S
+from bubbleensemble_implicitextension_b200 import workloads as W
+from tests.helpers import assert_bitwise, ragged_ensemble, run_gpu
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ["state", "uacc", "iuacc", "n_accepted", "n_rejected", "n_bicg_iter", "n_rhs", "status"]
+
+
+def bounded(ens, budget=50_000):
+    """Cap the attempted steps per period so that no test can run long."""
+    ens.max_steps_per_period = budget
+    return ens
+
+
+def test_c1_subset_two_periods_with_reset(gpu, oracle_lib):
+    ens = bounded(W.c1_ensemble().subset([0, 3, 7, 64, 100, 128, 200, 240, 250, 255]))
+    got = run_gpu(ens, n_periods=2, reset_at=1)
+    want = oracle_lib.run(ens, n_periods=2, reset_at=1)
+    assert_bitwise(got, want, KEYS)
+    assert (got["iuacc"] >= 0).any(), "no collapse was recorded"
+
+
+def test_ragged_sizes_one_launch_per_class(gpu, oracle_lib):
+    ens = bounded(ragged_ensemble([4, 8, 16, 20, 32, 33, 48, 64, 5, 31]))
+    got = run_gpu(ens, n_periods=1, reset_at=-1)
+    want = oracle_lib.run(ens, n_periods=1, reset_at=-1)
+    assert_bitwise(got, want, KEYS)
+
+
+def test_n128(gpu, oracle_lib):
+    ens = bounded(ragged_ensemble([128, 100], seed=5))
+    got = run_gpu(ens, n_periods=1, reset_at=-1)
+    want = oracle_lib.run(ens, n_periods=1, reset_at=-1)
+    assert_bitwise(got, want, KEYS)
+
+
+def test_solve_loop_equals_persistent_launch(gpu):
+    ens = bounded(W.c1_ensemble().subset([5, 77, 190]))
+    a = run_gpu(ens, n_periods=3, reset_at=2, per_period_solve=True)
+    b = run_gpu(ens, n_periods=3, reset_at=2)
+    assert_bitwise(a, b, KEYS)
+
+
+def test_rk4(gpu, oracle_lib):
+    ens = bounded(W.c1_ensemble().subset([20, 130]))
+    ens.dt0 = 2e-3
+    got = run_gpu(ens, n_periods=1, reset_at=-1, algorithm=S.Algorithms.RK4)
+    want = oracle_lib.run(ens, n_periods=1, reset_at=-1, algorithm=0)
+    assert_bitwise(got, want, KEYS)
+
+
+def test_dense_output(gpu, oracle_lib):
+    ens = bounded(W.c1_ensemble().subset([40, 41]))
+    got = run_gpu(ens, n_periods=2, reset_at=-1, ndo=24, do_min_dt=0.05, do_save_frequency=2)
+    want = oracle_lib.run(ens, n_periods=2, reset_at=-1, ndo=24, do_min_dt=0.05, do_save_frequency=2)
+    assert_bitwise(got, want, KEYS + ["dense_index", "dense_time", "dense_state"])
+    assert (got["dense_index"] == 24).all()
+
+
+def test_warps_per_block_does_not_change_results(gpu):
+    ens = bounded(W.c1_ensemble().subset(list(range(0, 256, 37))))
+    a = run_gpu(ens, n_periods=1, reset_at=-1, warps_per_block=1)
+    b = run_gpu(ens, n_periods=1, reset_at=-1, warps_per_block=4)
+    assert_bitwise(a, b, KEYS)
