@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""Benchmark: system-periods/s of the coupled Keller-Miksis ensemble integrator.
+
+Workload (default, ``c1_period1``): the plain-method ensemble of 256 systems
+(16 amplitudes 0.5-2 bar x 16 frequencies 20-200 kHz, log) of 32 coupled
+bubbles on a 1-D line (spacing 150 um, equilibrium radii U(2, 8) um, seeded),
+RKCK45 at rtol = atol = 1e-10, event location at dR/dt = 0 with collapse
+recording.  One step integrates one acoustic period of every system starting
+from rest (R = R_E, dR/dt = 0), i.e. 256 system-periods; every step starts
+again from rest so every step is the same work.  Later periods of this
+ensemble drive 74 of its 256 systems past 20k steps per period and one into
+the minimum step, where the reference solver (which has no step budget)
+cannot finish a period, so the shared workload is the first period.
+
+Arms:
+  --impl b200 (default): the sm_100a library through its C ABI.
+      value = device-resident throughput (inputs in HBM, CUDA events around
+      the solver launch on the solver's stream), e2e = the same through the
+      public API with host buffers (H2D of the step inputs, solve, D2H of the
+      results), roofline of the solver kernel against the measured FP64 FMA
+      throughput, cpu_baseline = the CPU oracle (OpenMP) on a bounded sample.
+  --impl reference: the reference's own per-block CUDA solver
+      (ProblemSolver, built unmodified for sm_100a by oracle/build_ref.py)
+      driven through its own API, same workload and metric.
+
+Multi-GPU (torchrun): every rank integrates its own full copy of the
+ensemble (weak scaling, no collective in the data path); the max over ranks
+of the timed region sets the time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "system-periods/sec at rtol 1e-10"
+UNIT = "system-periods/s"
+WORKLOAD = ("c1_period1: 256 systems (16 amplitudes 0.5-2 bar x 16 frequencies 20-200 kHz log) x 32 coupled "
+            "Keller-Miksis bubbles on a 1-D line (d = 150 um, R_E ~ U(2,8) um seed 1), RKCK45 rtol=atol=1e-10, "
+            "dt0=1e-3, dtmin=1e-13, events dR/dt=0 (dir -1, tol 1e-4) with collapse recording; one step = one "
+            "acoustic period of every system from rest")
+DATA = "synthetic: seeded PCG64 radii, reference parameter formulas (CollapseStrength.cu:329-357)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-systems", type=int, default=32)
+    ap.add_argument("--systems", type=int, default=256,
+                    help="profiling only: integrate every (256/S)-th system of the ensemble instead of all 256")
+    return ap.parse_args()
+
+
+def dist_init(n):
+    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return rank, world, int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def allreduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def flops_per_system(n, attempted, bicg):
+    """Algorithmic FP64 flops (FMA = 2): per attempted RKCK45 step 6 right-hand sides of
+    55N (Keller-Miksis) + 5N^2 + 5N (b and the first residual) plus 110N (stages and
+    controller); per completed BiCG iteration 6N^2 + 17N."""
+    rhs_base = 55 * n + 5 * n * n + 5 * n
+    return attempted * (6 * rhs_base + 110 * n) + bicg * (6 * n * n + 17 * n)
+
+
+def read_traffic():
+    """DRAM bytes per solver launch from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / "bes_ensemble_kernel_c1_period1.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_baseline(ens, n_sample):
+    from oracle import oracle as O
+    O.build()
+    systems = list(range(0, ens.n_systems, max(1, ens.n_systems // n_sample)))[:n_sample]
+    threads = O.max_threads()
+    t0 = time.perf_counter()
+    O.run(ens, n_periods=1, reset_at=-1, systems=systems, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": len(systems) / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"CPU oracle (C++ FP64, OpenMP {threads} threads): period 1 of {len(systems)} of the 256 "
+                      f"systems (every {ens.n_systems // len(systems)}th), {dt:.1f} s"}
+
+
+def run_b200(args, rank, world, local):
+    import torch
+
+    from bubbleensemble_implicitextension_b200 import solver as S
+    from bubbleensemble_implicitextension_b200 import workloads as W
+
+    V = S.ListOfVariables
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ens = W.c1_ensemble(n_periods=1, reset_at=-1)
+    if args.systems < ens.n_systems:
+        ens = ens.subset(list(range(0, ens.n_systems, ens.n_systems // args.systems))[:args.systems])
+    ens.max_steps_per_period = 1_000_000
+    ps = ens.make_solver(device=local)
+    stream = torch.cuda.current_stream(dev)
+    ps.set_stream(stream.cuda_stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
+    init_uacc, init_iuacc = ens.initial_uacc(), ens.initial_iuacc()
+
+    def load_inputs():
+        ps.set_array(V.ActualState, ens.state)
+        ps.set_array(V.UnitAccessories, init_uacc)
+        ps.set_array(V.IntegerUnitAccessories, init_iuacc)
+
+    load_inputs()
+    ps.SynchroniseFromHostToDevice(V.All)
+    torch.cuda.synchronize()
+
+    def device_step():
+        # untimed: the step's inputs back in HBM (rest state), then L2 flushed
+        ps.SynchroniseFromHostToDevice(V.ActualState)
+        ps.SynchroniseFromHostToDevice(V.UnitAccessories)
+        ps.SynchroniseFromHostToDevice(V.IntegerUnitAccessories)
+        ps.reset_counters()
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ps.solve_periods(1, -1)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), ps.last_solve_launches()
+
+    for _ in range(args.warmup):
+        device_step()
+    # timed region (device-resident inputs)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    times, launches = [], 0
+    for _ in range(args.steps):
+        ms, nl = device_step()
+        times.append(ms)
+        launches += nl
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier(world)
+    # counters of the last timed step (every step is identical work)
+    ps.SynchroniseFromDeviceToHost(V.Counters)
+    ps.InsertSynchronisationPoint()
+    ps.SynchroniseSolver()
+    c = ps.counters()
+    attempted = (c["accepted"] + c["rejected"]).astype(np.float64)
+    flops = float(sum(flops_per_system(int(n), a, b) for n, a, b in zip(ens.units, attempted, c["bicg"].astype(np.float64))))
+    total_ms = sum(times)
+    max_ms = allreduce_max(total_ms, world)
+    ms_per_step = max_ms / args.steps
+    value = world * ens.n_systems * args.steps / (max_ms * 1e-3)
+
+    # end to end through the public API: host inputs -> H2D -> solve -> D2H of the results
+    in_bytes = ens.state.nbytes + init_uacc.nbytes + init_iuacc.nbytes
+    out_bytes = in_bytes + 4 * 8 * ens.n_systems + 4 * ens.n_systems
+    e2e_times = []
+    for it in range(args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        load_inputs()
+        ps.SynchroniseFromHostToDevice(V.ActualState)
+        ps.SynchroniseFromHostToDevice(V.UnitAccessories)
+        ps.SynchroniseFromHostToDevice(V.IntegerUnitAccessories)
+        ps.solve_periods(1, -1)
+        ps.SynchroniseFromDeviceToHost(V.ActualState)
+        ps.SynchroniseFromDeviceToHost(V.UnitAccessories)
+        ps.SynchroniseFromDeviceToHost(V.IntegerUnitAccessories)
+        ps.SynchroniseFromDeviceToHost(V.Counters)
+        ps.InsertSynchronisationPoint()
+        ps.SynchroniseSolver()
+        _ = ps.get_array(V.UnitAccessories)
+        if it >= args.warmup:
+            e2e_times.append(time.perf_counter() - t0)
+    e2e_max = allreduce_max(sum(e2e_times), world)
+    e2e_value = world * ens.n_systems * args.steps / e2e_max
+    peak = S.measure_fp64_peak(local)
+    ps.close()
+    if rank != 0:
+        return None
+    kernel_s = total_ms * 1e-3 / args.steps
+    achieved = flops / kernel_s / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": DATA,
+        "config": {"workload": WORKLOAD, "systems": ens.n_systems, "units_per_system": 32,
+                   "periods_per_step": 1, "l2": "flushed between timed steps (256 MiB write, untimed)",
+                   "parallelism": f"{world} independent ensemble replica(s), one per GPU"},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None, "traffic": read_traffic(),
+                     "peak_source": "measured live: bes_measure_fp64_peak FMA-throughput loop (no FP64 figure in "
+                                    "MEASURED_PEAKS.json)",
+                     "flops_per_launch": flops, "kernel": "bes::bes_ensemble_kernel<1>"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(in_bytes),
+                "d2h_bytes_per_step": int(out_bytes)},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "counters": {"attempted_steps": int(attempted.sum()), "max_attempted_steps": int(attempted.max()),
+                     "bicg_iterations": int(c["bicg"].sum()), "status_or": int(np.bitwise_or.reduce(c["status"]))},
+    }
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(ens, args.cpu_sample_systems)
+    return line
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    from bubbleensemble_implicitextension_b200 import workloads as W
+    from oracle import build_ref, ref_io
+
+    exe = build_ref.path(32, 256, 0, True)
+    if not exe.exists():
+        return {"impl": "reference", "unavailable": f"{exe.name} was not built (the reference tree was absent at build time)"}
+    ens = W.c1_ensemble(n_periods=1, reset_at=-1)
+    n = args.warmup + args.steps
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    out = ref_io.run(exe, ens, n, -1, ROOT / "gpurun_out" / "ref_bench", tag="bench", timeout=3600,
+                     restart_each_period=True)
+    clk = clocks.stop()
+    per = out["period_s"][args.warmup:]
+    value = ens.n_systems * len(per) / per.sum()
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * per.mean(), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": DATA, "impl": "reference",
+        "config": {"workload": WORKLOAD, "systems": ens.n_systems, "units_per_system": 32, "periods_per_step": 1,
+                   "l2": "inputs re-set through SetHost + SynchroniseFromHostToDevice before every period (untimed)",
+                   "parallelism": "reference ProblemSolver, one GPU"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "kind": "reference", "cores": 1,
+                         "sample": "the reference's own per-block CUDA solver (ProblemSolver<256,32,...,RKCK45,double>, "
+                                   "unmodified headers, nvcc -O3 -maxrregcount=128 sm_100a) on the same GPU, "
+                                   "timed per Solve() with the host thread waiting on its event; the reference "
+                                   "has no CPU implementation"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clk,
+    }
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_init(args.gpus)
+    line = run_reference(args, rank, world) if args.impl == "reference" else run_b200(args, rank, world, local)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -172,6 +172,7 @@ SIGNATURES = {
     "bes_load_bubble_sizes": [ctypes.c_char_p, _I32, _DP],
     "bes_load_coupling_matrix": [ctypes.c_char_p, _I32, _DP],
     "bes_device_count": [ctypes.POINTER(ctypes.c_int32)],
+    "bes_measure_fp64_peak": [_I32, ctypes.POINTER(ctypes.c_double)],
     "bes_status_string": [_I32],
     "bes_last_error": [_P],
 }
@@ -209,6 +210,14 @@ def device_count() -> int:
     n = ctypes.c_int32(0)
     st = lib.bes_device_count(ctypes.byref(n))
     return n.value if st == 0 else 0
+
+
+def measure_fp64_peak(device: int = 0) -> float:
+    """FP64 FMA throughput of the device in TFLOP/s (bes_measure_fp64_peak)."""
+    lib = load_library()
+    t = ctypes.c_double()
+    _check(lib, None, lib.bes_measure_fp64_peak(device, ctypes.byref(t)))
+    return t.value
 
 
 def _check(lib, handle, status: int) -> None:

@@ -235,6 +235,12 @@ bes_status bes_load_coupling_matrix(const char* path, int32_t n, double* out);
 /* ListCUDADevices, Interface.cuh:260-311 */
 bes_status bes_device_count(int32_t* count);
 
+/* Utility, no reference counterpart: the device's FP64 fused multiply-add
+ * throughput in TFLOP/s (2 flops per FMA), measured with an FMA loop that
+ * keeps 8 independent chains per thread on every SM; the roofline
+ * denominator of the FP64 solver kernel. */
+bes_status bes_measure_fp64_peak(int32_t device, double* tflops);
+
 const char* bes_status_string(bes_status status);
 const char* bes_last_error(const bes_solver* h);
 

@@ -94,6 +94,7 @@ int main(int argc, char** argv) {
     if (hdr[0] != MAGIC_IN) die("bad input magic");
     const int ns = (int)hdr[1], ups = (int)hdr[2], ndo = (int)hdr[3], n_periods = (int)hdr[4], reset_at = (int)hdr[5];
     const int evdir = (int)hdr[6], do_freq = (int)hdr[7], device = (int)hdr[8];
+    const int restart_each_period = (int)hdr[9]; /* 1: every period starts again from the input state */
     if (ups != UPS) die("unit count differs from the compiled HARNESS_UPS");
     if (ndo != NDO) die("dense-output slots differ from the compiled HARNESS_NDO");
     if (ns < 1 || ns > NS) die("system count outside 1..HARNESS_NS");
@@ -151,8 +152,24 @@ int main(int argc, char** argv) {
     S.SynchroniseFromHostToDevice(All);
     S.InsertSynchronisationPoint();
     S.SynchroniseSolver();
+    std::vector<double> period_s(n_periods, 0.0);
     auto t0 = std::chrono::steady_clock::now();
     for (int p = 0; p < n_periods; p++) {
+        if (restart_each_period && p > 0) {
+            /* the same period again from the input state: SetHost + H2D of the unit-scope state */
+            for (int sid = 0; sid < ns; sid++)
+                for (int uid = 0; uid < UPS; uid++) {
+                    const int64_t u = (int64_t)sid * ups + uid;
+                    for (int k = 0; k < UD; k++) S.SetHost(sid, uid, ActualState, k, state[k * tu + u]);
+                    for (int k = 0; k < NUA; k++) S.SetHost(sid, uid, UnitAccessories, k, uacc[k * tu + u]);
+                    S.SetHost(sid, uid, IntegerUnitAccessories, 0, iuacc[u]);
+                }
+            S.SynchroniseFromHostToDevice(ActualState);
+            S.SynchroniseFromHostToDevice(UnitAccessories);
+            S.SynchroniseFromHostToDevice(IntegerUnitAccessories);
+            S.InsertSynchronisationPoint();
+            S.SynchroniseSolver();
+        }
         if (p == reset_at) {
             /* ResetAccessories, CollapseStrength.cu:373-396 */
             for (int sid = 0; sid < NS; sid++)
@@ -163,9 +180,11 @@ int main(int argc, char** argv) {
             S.SynchroniseFromHostToDevice(UnitAccessories);
             S.SynchroniseFromHostToDevice(IntegerUnitAccessories);
         }
+        auto tp = std::chrono::steady_clock::now();
         S.Solve();
         S.InsertSynchronisationPoint();
         S.SynchroniseSolver();
+        period_s[p] = std::chrono::duration<double>(std::chrono::steady_clock::now() - tp).count();
     }
     auto t1 = std::chrono::steady_clock::now();
     S.SynchroniseFromDeviceToHost(All);
@@ -208,6 +227,7 @@ int main(int argc, char** argv) {
         wr(fo, o_dt.data(), o_dt.size());
         wr(fo, o_ds.data(), o_ds.size());
     }
+    wr(fo, period_s.data(), period_s.size());
     std::fclose(fo);
     std::printf("ref_harness: %d systems x %d units, %d periods, %.6f s\n", ns, ups, n_periods,
                 (double)oh[4] * 1e-9);

@@ -1,14 +1,16 @@
 """TEST INFRASTRUCTURE: input/output files of oracle/ref_harness.cu.
 
 Input (little endian): int64 header[16] = {magic "BESRFIN1", n_systems, units,
-ndo, n_periods, reset_at, event_dir, do_save_frequency, device, 0...};
+ndo, n_periods, reset_at, event_dir, do_save_frequency, device,
+restart_each_period, 0...};
 double options[16] = {dt0, dtmin, dtmax, rtol0, rtol1, atol0, atol1,
 event_tol, grow, shrink, do_min_dt, 0...}; then upar [21][TU], state [2][TU],
 uacc [64][TU] (double), iuacc [TU] (int32) and the N x N column-major
 coupling matrix.  Output: int64 header[8] = {magic "BESRFOU1", n_systems,
 units, ndo, elapsed_ns, n_periods, 0, 0}; state [2][TU], uacc [64][TU],
 iuacc [TU], actual_time [NS], dense_index [NS] and, when ndo > 0,
-dense_time [ndo][NS] and dense_state [ndo][2][TU].
+dense_time [ndo][NS] and dense_state [ndo][2][TU]; then the seconds of each
+period's Solve() + synchronisation [n_periods].
 """
 from __future__ import annotations
 
@@ -22,12 +24,14 @@ MAGIC_OUT = 0x42455352464f5531
 
 
 def write_input(path, ens, n_periods: int, reset_at: int, ndo: int = 0, do_min_dt: float = 0.0,
-                do_save_frequency: int = 1, device: int = 0, uacc=None, iuacc=None) -> None:
+                do_save_frequency: int = 1, device: int = 0, uacc=None, iuacc=None,
+                restart_each_period: bool = False) -> None:
     if len(set(ens.units.tolist())) != 1 or ens.n_matrices != 1:
         raise ValueError("the reference solver needs one unit count and one shared coupling matrix")
     ns, n = ens.n_systems, int(ens.units[0])
     hdr = np.zeros(16, np.int64)
-    hdr[:9] = [MAGIC_IN, ns, n, ndo, n_periods, reset_at, ens.event_dir, do_save_frequency, device]
+    hdr[:10] = [MAGIC_IN, ns, n, ndo, n_periods, reset_at, ens.event_dir, do_save_frequency, device,
+                int(restart_each_period)]
     opt = np.zeros(16)
     opt[:11] = [ens.dt0, ens.dtmin, ens.dtmax, ens.rtol[0, 0], ens.rtol[1, 0], ens.atol[0, 0], ens.atol[1, 0],
                 ens.event_tol, ens.grow, ens.shrink, do_min_dt]
@@ -65,6 +69,7 @@ def read_output(path) -> dict:
     if ndo:
         out["dense_time"] = take(ndo * ns, np.float64).reshape(ndo, ns)
         out["dense_state"] = take(ndo * 2 * tu, np.float64).reshape(ndo, 2, tu)
+    out["period_s"] = take(out["n_periods"], np.float64)
     return out
 
 
