@@ -91,6 +91,7 @@ struct bes_solver {
     /* launch plan */
     bool order_dirty = true;
     int class_begin[3] = {0, 0, 0}, class_count[3] = {0, 0, 0};
+    bool class0_all32 = false;
     int sm_count = 148;
     float last_ms = 0.f;
     int last_launches = 0;
@@ -233,6 +234,9 @@ bes_status build_order(bes_solver* h) {
         while (pos < nact && units_class(h->units[idx[pos]]) == c) pos++;
         h->class_count[c] = pos - h->class_begin[c];
     }
+    h->class0_all32 = true;
+    for (int i = 0; i < h->class_count[0]; i++)
+        if (h->units[idx[i]] != 32) h->class0_all32 = false;
     if (nact > 0)
         CUDA_TRY(h, cudaMemcpyAsync(h->d_order, h->h_order, sizeof(int32_t) * nact, cudaMemcpyHostToDevice, h->stream));
     h->order_dirty = false;
@@ -289,6 +293,8 @@ DeviceProblem make_problem(bes_solver* h) {
 
 bes_status launch_class(bes_solver* h, DeviceProblem P, int cls) {
     const int U = cls == 0 ? 1 : (cls == 1 ? 2 : 4);
+    /* N <= 32: operator in registers (2: every system has exactly 32 units) */
+    const int rhs = cls == 0 ? (h->class0_all32 ? 2 : 1) : 0;
     const int count = h->class_count[cls];
     if (count == 0) return BES_OK;
     P.order = h->d_order + h->class_begin[cls];
@@ -303,12 +309,12 @@ bes_status launch_class(bes_solver* h, DeviceProblem P, int cls) {
     const int max_wpb_smem = (227 * 1024) / smem_warp;
     wpb = std::max(1, std::min(std::min(wpb, 4), max_wpb_smem));
     int per_sm = 0;
-    CUDA_TRY(h, bes::occupancy(U, wpb, &per_sm));
+    CUDA_TRY(h, bes::occupancy(U, rhs, wpb, &per_sm));
     if (per_sm < 1)
         return fail(h, BES_ERR_CUDA, "solver kernel (U=%d) cannot be resident with %d warps per block", U, wpb);
     const int needed = (count + wpb - 1) / wpb;
     const int grid = std::max(1, std::min(needed, per_sm * h->sm_count));
-    CUDA_TRY(h, bes::launch(U, P, grid, wpb, h->stream));
+    CUDA_TRY(h, bes::launch(U, rhs, P, grid, wpb, h->stream));
     h->last_launches++;
     return BES_OK;
 }
@@ -938,7 +944,7 @@ bes_status bes_set_stream(bes_solver* h, void* cuda_stream) {
     bes_status st = check_solver(h);
     if (st) return st;
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-    h->stream = cuda_stream ? (cudaStream_t)cuda_stream : h->own_stream;
+    h->stream = (cudaStream_t)cuda_stream; /* NULL: the legacy default stream */
     return BES_OK;
 }
 

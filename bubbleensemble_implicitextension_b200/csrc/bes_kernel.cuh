@@ -63,15 +63,19 @@ constexpr int NSAa = NSA > 0 ? NSA : 1;
 constexpr int NISAa = NISA > 0 ? NISA : 1;
 constexpr unsigned FULL = 0xffffffffu;
 
-/* shared-memory doubles per warp for U units per lane */
+/* Shared-memory doubles per warp for U units per lane: one NMAX x (NMAX+1)
+ * matrix region (the operator W with the shared-memory operator, the system's
+ * coupling matrix C with the register-resident operator), six broadcast
+ * vectors and the system-scope arrays. */
 template <int U>
 struct WarpSmem {
     static constexpr int NMAX = 32 * U;
     static constexpr int LDW = NMAX + 1;
     static constexpr int W_DOUBLES = NMAX * LDW;
-    static constexpr int VEC_DOUBLES = 5 * NMAX;
+    static constexpr int VEC_DOUBLES = 6 * NMAX;
     static constexpr int SYS_DOUBLES = NSPa + NSAa + NISAa; /* ints stored in double slots */
-    static constexpr int DOUBLES = W_DOUBLES + VEC_DOUBLES + SYS_DOUBLES;
+    static constexpr int UP_DOUBLES = NMAX * NUPa;          /* unit parameters, lane-contiguous */
+    static constexpr int DOUBLES = W_DOUBLES + VEC_DOUBLES + SYS_DOUBLES + UP_DOUBLES;
     static constexpr int BYTES = DOUBLES * 8;
 };
 
@@ -131,9 +135,10 @@ template <int U>
 struct Sys {
     int lane, sid, N;
     int64_t off, tot;
-    const double* C;
-    double* W;
-    double *vp, *vpt, *vcpt, *vx1, *vxu;
+    const double* C;   /* the system's coupling matrix in HBM */
+    double* W;         /* matrix region in shared memory: W, or a padded copy of C */
+    double *vp, *vpt, *vcpt, *vx1, *vxu, *vrd;
+    double* upsh;      /* unit parameters of the register-operator variant: unit i at upsh[i * NUP] */
     double* sPAR;
     double* sACC;
     int* isACC;
@@ -290,6 +295,137 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U>& S, const DeviceProblem&
     return done;
 }
 
+/* ---------------------------------------------------------------------------
+ * Coupled right-hand side with the operator in registers (N <= 32, one unit
+ * per lane).  Lane i holds row i of W (for A p) and column i of W (for
+ * A^T p~) as 64 doubles; the system's coupling matrix sits in shared memory
+ * (padded, leading dimension 33: row and column reads are conflict-free),
+ * staged once per system.  NFIX = 32 drops the N guards for full warps.
+ * Same arithmetic, in the same order, as the shared-memory variant. */
+template <int NFIX>
+__device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DeviceProblem& P, double T,
+                                                double (&Xs)[1][UD], double (&F)[1][UD],
+                                                double (&up)[1][NUPa], double (&ua)[1][NUAa],
+                                                int (&iua)[1][NIUAa], bool& capped) {
+    constexpr int LDC = WarpSmem<1>::LDW;
+    const int N = NFIX ? NFIX : S.N;
+    const int i = S.lane;
+    const bool valid = i < N;
+    double xu = 0.0, rd = 0.0, x1 = 0.0;
+    __syncwarp();
+    if (valid) {
+        double Fl[UD], cpt, cpf;
+        CoupledSystems_PerBlock_OdeFunction<double>(S.sid, i, Fl, Xs[0], T, S.upsh + i * NUPa, S.sPAR, S.gPAR,
+                                                    S.igPAR, ua[0], iua[0], S.sACC, S.isACC, &cpt, &cpf);
+#pragma unroll
+        for (int k = 0; k < UD; k++) F[0][k] = Fl[k];
+        xu = Fl[IC];
+        rd = cpf;
+        x1 = Xs[0][0] * Xs[0][0];
+        S.vcpt[i] = cpt;
+    } else {
+#pragma unroll
+        for (int k = 0; k < UD; k++) F[0][k] = 0.0;
+        S.vcpt[i] = 0.0;
+    }
+    S.vx1[i] = x1;
+    S.vxu[i] = xu;
+    S.vrd[i] = rd;
+    __syncwarp();
+    double wr[32], wc[32];
+    double b = 0.0, ax = 0.0;
+    const double* Crow = S.W + i;        /* C[i][j] at i + j*LDC */
+    const double* Ccol = S.W + i * LDC;  /* C[j][i] at j + i*LDC */
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+        const double cij = Crow[j * LDC];
+        const double cji = Ccol[j];
+        const double x1j = S.vx1[j];
+        const bool in = NFIX != 0 || j < N;
+        if (in) {
+            b = fma(cij, S.vcpt[j], b);
+            ax = fma(cij * x1j, S.vxu[j], ax);
+        }
+        wr[j] = in ? (rd * cij) * x1j : 0.0;
+        wc[j] = in ? (S.vrd[j] * cji) * x1 : 0.0;
+    }
+    double r = 0.0;
+    if (valid) {
+        b = fma(rd, b, xu);
+        ax = fma(rd, ax, xu);
+        r = b - ax;
+    }
+    double rt = r, x = xu, p = 0.0, pt = 0.0;
+    double prod[1] = {r * rt};
+    double rho1 = warp_tree_sum<1>(prod);
+    double rho2 = 0.0;
+    int done = 0;
+    bool exited = false;
+    const double2* vp2 = reinterpret_cast<const double2*>(S.vp);
+    const double2* vpt2 = reinterpret_cast<const double2*>(S.vpt);
+    for (int iter = 1; iter <= P.bicg_max_iter; iter++) {
+        if (iter == 1) {
+            p = r;
+            pt = rt;
+            if (fabs(rho1) < 1e-6) { exited = true; break; }
+        } else {
+            const double beta = rho1 / rho2;
+            p = fma(beta, p, r);
+            pt = fma(beta, pt, rt);
+        }
+        __syncwarp();
+        S.vp[i] = p;
+        S.vpt[i] = pt;
+        __syncwarp();
+        double q = p;
+#pragma unroll
+        for (int j = 0; j < 32; j += 2) {
+            const double2 a = vp2[j / 2];
+            if (NFIX != 0 || j < N) q = fma(wr[j], a.x, q);
+            if (NFIX != 0 || j + 1 < N) q = fma(wr[j + 1], a.y, q);
+        }
+        /* first tree level t_k + t_{k+16} on the loads, then the halving tree over 16 */
+        double u[16];
+#pragma unroll
+        for (int k = 0; k < 16; k += 2) {
+            const double2 lo = vpt2[k / 2], hi = vpt2[(k + 16) / 2];
+            u[k] = wc[k] * lo.x + wc[k + 16] * hi.x;
+            u[k + 1] = wc[k + 1] * lo.y + wc[k + 17] * hi.y;
+        }
+        auto leaf = [&](int k) -> double { return u[k]; };
+        double qt = pt + TreeSum<1, 16>::run(0, leaf);
+        if (!valid) { q = 0.0; qt = 0.0; }
+        prod[0] = pt * q;
+        const double alpha = rho1 / warp_tree_sum<1>(prod);
+        x = fma(alpha, p, x);
+        r = fma(-alpha, q, r);
+        rt = fma(-alpha, qt, rt);
+        double ar[1] = {fabs(r)};
+        const double rmax = warp_tree_max<1>(ar);
+        rho2 = rho1;
+        done++;
+        if (rmax < 1e-6) { exited = true; break; }
+        prod[0] = r * rt;
+        rho1 = warp_tree_sum<1>(prod);
+    }
+    if (!exited) capped = true;
+    F[0][IC] = x;
+    return done;
+}
+
+/* the right-hand side a kernel variant uses */
+template <int U, int RHS>
+__device__ __forceinline__ int rhs_eval(const Sys<U>& S, const DeviceProblem& P, double T, double (&Xs)[U][UD],
+                                        double (&F)[U][UD], double (&up)[U][NUPa], double (&ua)[U][NUAa],
+                                        int (&iua)[U][NIUAa], bool& capped) {
+    if constexpr (RHS == 0) {
+        return coupled_rhs<U>(S, P, T, Xs, F, up, ua, iua, capped);
+    } else {
+        static_assert(U == 1, "the register-resident operator needs one unit per lane");
+        return coupled_rhs_regw<RHS == 2 ? 32 : 0>(S, P, T, Xs, F, up, ua, iua, capped);
+    }
+}
+
 /* per-lane state of the units it owns */
 template <int U>
 struct Lane {
@@ -308,62 +444,74 @@ struct Counters {
 template <int U>
 __device__ __forceinline__ bool valid_unit(const Sys<U>& S, int m) { return S.lane + 32 * m < S.N; }
 
+/* the parameter array a callback gets for slot m of this lane */
+template <int U, int RHS>
+__device__ __forceinline__ double* upar_of(const Sys<U>& S, Lane<U>& L, int m) {
+    if constexpr (RHS != 0) return S.upsh + (S.lane + 32 * m) * NUPa;
+    else return L.up[m];
+}
+
+/* Cash-Karp tableau (Steppers.cuh:197-370): stage nodes and coefficients,
+ * each entry the double nearest to the reference's literal fraction. */
+__constant__ double kCK_A[6][5] = {
+    {0.0, 0.0, 0.0, 0.0, 0.0},
+    {1.0 / 5.0, 0.0, 0.0, 0.0, 0.0},
+    {3.0 / 40.0, 9.0 / 40.0, 0.0, 0.0, 0.0},
+    {3.0 / 10.0, -9.0 / 10.0, 6.0 / 5.0, 0.0, 0.0},
+    {-11.0 / 54.0, 5.0 / 2.0, -70.0 / 27.0, 35.0 / 27.0, 0.0},
+    {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0}};
+__constant__ double kCK_C[6] = {0.0, 1.0 / 5.0, 3.0 / 10.0, 3.0 / 5.0, 1.0, 7.0 / 8.0};
+/* classical RK4 */
+__constant__ double kRK4_A[4] = {0.0, 0.5, 0.5, 1.0};
+
 /* ---------------------------------------------------------------------------
- * RKCK45 step (Steppers.cuh:94-425); returns finiteness of y5 and the error */
-template <int U>
+ * RKCK45 step (Steppers.cuh:94-425); returns finiteness of y5 and the error.
+ * The six stages run as one loop so the coupled right-hand side is inlined
+ * once; stage s evaluates at X + dt * (sum_j<s a_sj K_j) with the terms
+ * accumulated in the reference's order (first a product, then fmas). */
+template <int U, int RHS>
 __device__ __forceinline__ bool step_rkck45(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L,
                                             double T, double dt, double (&Yn)[U][UD], double (&E)[U][UD],
                                             Counters& cnt, bool& capped) {
     double K[6][U][UD];
-    double Xs[U][UD];
-    cnt.bicg += coupled_rhs<U>(S, P, T, L.X, K[0], L.up, L.ua, L.iua, capped);
 #pragma unroll
-    for (int m = 0; m < U; m++)
+    for (int j = 0; j < 6; j++)
 #pragma unroll
-        for (int c = 0; c < UD; c++) Xs[m][c] = fma(K[0][m][c] * (1.0 / 5.0), dt, L.X[m][c]);
-    cnt.bicg += coupled_rhs<U>(S, P, fma(1.0 / 5.0, dt, T), Xs, K[1], L.up, L.ua, L.iua, capped);
+        for (int m = 0; m < U; m++)
 #pragma unroll
-    for (int m = 0; m < U; m++)
+            for (int c = 0; c < UD; c++) K[j][m][c] = 0.0;
+#pragma unroll 1
+    for (int st = 0; st < 6; st++) {
+        double Xs[U][UD], F[U][UD];
+        double Ts;
+        if (st == 0) {
+            Ts = T;
 #pragma unroll
-        for (int c = 0; c < UD; c++) {
-            double s = K[0][m][c] * (3.0 / 40.0);
-            s = fma(K[1][m][c], 9.0 / 40.0, s);
-            Xs[m][c] = fma(s, dt, L.X[m][c]);
+            for (int m = 0; m < U; m++)
+#pragma unroll
+                for (int c = 0; c < UD; c++) Xs[m][c] = L.X[m][c];
+        } else {
+            Ts = st == 4 ? T + dt : fma(kCK_C[st], dt, T);
+#pragma unroll
+            for (int m = 0; m < U; m++)
+#pragma unroll
+                for (int c = 0; c < UD; c++) {
+                    double acc = K[0][m][c] * kCK_A[st][0];
+#pragma unroll
+                    for (int j = 1; j < 5; j++)
+                        if (j < st) acc = fma(K[j][m][c], kCK_A[st][j], acc);
+                    Xs[m][c] = fma(acc, dt, L.X[m][c]);
+                }
         }
-    cnt.bicg += coupled_rhs<U>(S, P, fma(3.0 / 10.0, dt, T), Xs, K[2], L.up, L.ua, L.iua, capped);
+        cnt.bicg += rhs_eval<U, RHS>(S, P, Ts, Xs, F, L.up, L.ua, L.iua, capped);
 #pragma unroll
-    for (int m = 0; m < U; m++)
+        for (int j = 0; j < 6; j++)
 #pragma unroll
-        for (int c = 0; c < UD; c++) {
-            double s = K[0][m][c] * (3.0 / 10.0);
-            s = fma(K[1][m][c], -9.0 / 10.0, s);
-            s = fma(K[2][m][c], 6.0 / 5.0, s);
-            Xs[m][c] = fma(s, dt, L.X[m][c]);
-        }
-    cnt.bicg += coupled_rhs<U>(S, P, fma(3.0 / 5.0, dt, T), Xs, K[3], L.up, L.ua, L.iua, capped);
+            for (int m = 0; m < U; m++)
 #pragma unroll
-    for (int m = 0; m < U; m++)
-#pragma unroll
-        for (int c = 0; c < UD; c++) {
-            double s = K[0][m][c] * (-11.0 / 54.0);
-            s = fma(K[1][m][c], 5.0 / 2.0, s);
-            s = fma(K[2][m][c], -70.0 / 27.0, s);
-            s = fma(K[3][m][c], 35.0 / 27.0, s);
-            Xs[m][c] = fma(s, dt, L.X[m][c]);
-        }
-    cnt.bicg += coupled_rhs<U>(S, P, T + dt, Xs, K[4], L.up, L.ua, L.iua, capped);
-#pragma unroll
-    for (int m = 0; m < U; m++)
-#pragma unroll
-        for (int c = 0; c < UD; c++) {
-            double s = K[0][m][c] * (1631.0 / 55296.0);
-            s = fma(K[1][m][c], 175.0 / 512.0, s);
-            s = fma(K[2][m][c], 575.0 / 13824.0, s);
-            s = fma(K[3][m][c], 44275.0 / 110592.0, s);
-            s = fma(K[4][m][c], 253.0 / 4096.0, s);
-            Xs[m][c] = fma(s, dt, L.X[m][c]);
-        }
-    cnt.bicg += coupled_rhs<U>(S, P, fma(7.0 / 8.0, dt, T), Xs, K[5], L.up, L.ua, L.iua, capped);
+                for (int c = 0; c < UD; c++)
+                    if (j == st) K[j][m][c] = F[m][c];
+    }
     cnt.rhs += 6;
     bool finite = true;
 #pragma unroll
@@ -388,27 +536,49 @@ __device__ __forceinline__ bool step_rkck45(const Sys<U>& S, const DeviceProblem
 
 /* classical RK4 step (the reference has only its fixed-step controller,
  * ErrorControllers.cuh:424-450) */
-template <int U>
+template <int U, int RHS>
 __device__ __forceinline__ bool step_rk4(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L,
                                          double T, double dt, double (&Yn)[U][UD], Counters& cnt, bool& capped) {
     double K[4][U][UD];
-    double Xs[U][UD];
-    cnt.bicg += coupled_rhs<U>(S, P, T, L.X, K[0], L.up, L.ua, L.iua, capped);
 #pragma unroll
-    for (int m = 0; m < U; m++)
+    for (int j = 0; j < 4; j++)
 #pragma unroll
-        for (int c = 0; c < UD; c++) Xs[m][c] = fma(K[0][m][c] * 0.5, dt, L.X[m][c]);
-    cnt.bicg += coupled_rhs<U>(S, P, fma(0.5, dt, T), Xs, K[1], L.up, L.ua, L.iua, capped);
+        for (int m = 0; m < U; m++)
 #pragma unroll
-    for (int m = 0; m < U; m++)
+            for (int c = 0; c < UD; c++) K[j][m][c] = 0.0;
+#pragma unroll 1
+    for (int st = 0; st < 4; st++) {
+        double Xs[U][UD], F[U][UD];
+        double Ts;
+        if (st == 0) {
+            Ts = T;
 #pragma unroll
-        for (int c = 0; c < UD; c++) Xs[m][c] = fma(K[1][m][c] * 0.5, dt, L.X[m][c]);
-    cnt.bicg += coupled_rhs<U>(S, P, fma(0.5, dt, T), Xs, K[2], L.up, L.ua, L.iua, capped);
+            for (int m = 0; m < U; m++)
 #pragma unroll
-    for (int m = 0; m < U; m++)
+                for (int c = 0; c < UD; c++) Xs[m][c] = L.X[m][c];
+        } else {
+            Ts = st == 3 ? T + dt : fma(0.5, dt, T);
 #pragma unroll
-        for (int c = 0; c < UD; c++) Xs[m][c] = fma(K[2][m][c], dt, L.X[m][c]);
-    cnt.bicg += coupled_rhs<U>(S, P, T + dt, Xs, K[3], L.up, L.ua, L.iua, capped);
+            for (int m = 0; m < U; m++)
+#pragma unroll
+                for (int c = 0; c < UD; c++) {
+                    double kprev = 0.0;
+#pragma unroll
+                    for (int j = 0; j < 3; j++)
+                        if (j == st - 1) kprev = K[j][m][c];
+                    /* stage 3 uses K3 itself (a = 1): fma(K3, dt, X); stages 1, 2 use K*0.5 */
+                    Xs[m][c] = st == 3 ? fma(kprev, dt, L.X[m][c]) : fma(kprev * kRK4_A[st], dt, L.X[m][c]);
+                }
+        }
+        cnt.bicg += rhs_eval<U, RHS>(S, P, Ts, Xs, F, L.up, L.ua, L.iua, capped);
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int m = 0; m < U; m++)
+#pragma unroll
+                for (int c = 0; c < UD; c++)
+                    if (j == st) K[j][m][c] = F[m][c];
+    }
     cnt.rhs += 4;
     bool finite = true;
 #pragma unroll
@@ -452,7 +622,7 @@ __device__ __forceinline__ void store_dense(const Sys<U>& S, const DeviceProblem
 
 /* ---------------------------------------------------------------------------
  * One reference Solve() of one system (Solver.cuh:82-648). */
-template <int U>
+template <int U, int RHS>
 __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, Counters& cnt,
                            double (&TD)[2], double& T, int& do_idx) {
     const double TD1 = TD[1];
@@ -484,7 +654,7 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
             if (i < S.N) {
                 double Tu = Tl, dTu = dTl;
                 int DOu = DOl;
-                CoupledSystems_PerBlock_Initialization<double>(S.sid, i, DOu, Tu, dTu, TD, L.X[m], L.up[m], S.sPAR,
+                CoupledSystems_PerBlock_Initialization<double>(S.sid, i, DOu, Tu, dTu, TD, L.X[m], upar_of<U, RHS>(S, L, m), S.sPAR,
                                                                S.gPAR, S.igPAR, L.ua[m], L.iua[m], S.sACC, S.isACC);
                 if (firstT < 0 && Tu != Tl) { firstT = i; TnewL = Tu; }
                 if (firstD < 0 && dTu != dTl) { firstD = i; dTnewL = dTu; }
@@ -502,7 +672,7 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
         for (int m = 0; m < U; m++)
             if (valid_unit(S, m))
                 CoupledSystems_PerBlock_EventFunction<double>(S.sid, S.lane + 32 * m, L.ev_a[m], T, dt, TD, L.X[m],
-                                                              L.up[m], S.sPAR, S.gPAR, S.igPAR, L.ua[m], L.iua[m],
+                                                              upar_of<U, RHS>(S, L, m), S.sPAR, S.gPAR, S.igPAR, L.ua[m], L.iua[m],
                                                               S.sACC, S.isACC);
     }
     if (P.ndo > 0) store_dense<U>(S, P, L, do_idx, update_do, 1, skipped, do_time, T, TD1);
@@ -519,7 +689,7 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
         double Yn[U][UD], E[U][UD];
         bool finite;
         if (P.algorithm == 1) {
-            finite = step_rkck45<U>(S, P, L, T, dt, Yn, E, cnt, capped);
+            finite = step_rkck45<U, RHS>(S, P, L, T, dt, Yn, E, cnt, capped);
             /* ErrorController_RKCK45 (ErrorControllers.cuh:454-542) */
             double rr = 1e30;
             int ru = 1;
@@ -553,7 +723,7 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
             newdt = fmin(newdt, P.dtmax);
             newdt = fmax(newdt, P.dtmin);
         } else {
-            finite = step_rk4<U>(S, P, L, T, dt, Yn, cnt, capped);
+            finite = step_rk4<U, RHS>(S, P, L, T, dt, Yn, cnt, capped);
             if (!finite) { cnt.status |= BES_STATUS_NONFINITE; terminate = true; update = 0; }
             newdt = P.dt0;
         }
@@ -565,7 +735,7 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
             for (int m = 0; m < U; m++)
                 if (valid_unit(S, m))
                     CoupledSystems_PerBlock_EventFunction<double>(S.sid, S.lane + 32 * m, L.ev_n[m], T + dt, newdt, TD,
-                                                                  Yn[m], L.up[m], S.sPAR, S.gPAR, S.igPAR, L.ua[m],
+                                                                  Yn[m], upar_of<U, RHS>(S, L, m), S.sPAR, S.gPAR, S.igPAR, L.ua[m],
                                                                   L.iua[m], S.sACC, S.isACC);
             if (update == 1) {
                 /* EventTimeStepControl (EventHandling.cuh:216-268) */
@@ -617,7 +787,7 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
                         double Tu = Tl, dTu = dTl;
                         int Uu = udt;
                         CoupledSystems_PerBlock_ActionAfterSuccessfulTimeStep<double>(
-                            S.sid, i, Uu, Tu, dTu, TD, L.X[m], L.up[m], S.sPAR, S.gPAR, S.igPAR, L.ua[m], L.iua[m],
+                            S.sid, i, Uu, Tu, dTu, TD, L.X[m], upar_of<U, RHS>(S, L, m), S.sPAR, S.gPAR, S.igPAR, L.ua[m], L.iua[m],
                             S.sACC, S.isACC);
                         if (firstT < 0 && Tu != Tl) { firstT = i; TnewL = Tu; }
                         if (firstD < 0 && dTu != dTl) { firstD = i; dTnewL = dTu; }
@@ -645,7 +815,7 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
                                 double Tu = Tl, dTu = dTl;
                                 int Uu = udt;
                                 CoupledSystems_PerBlock_ActionAfterEventDetection<double>(
-                                    S.sid, i, e, Uu, Tu, dTu, TD, L.X[m], L.up[m], S.sPAR, S.gPAR, S.igPAR, L.ua[m],
+                                    S.sid, i, e, Uu, Tu, dTu, TD, L.X[m], upar_of<U, RHS>(S, L, m), S.sPAR, S.gPAR, S.igPAR, L.ua[m],
                                     L.iua[m], S.sACC, S.isACC);
                                 if (firstT < 0 && Tu != Tl) { firstT = i; TnewL = Tu; }
                                 if (firstD < 0 && dTu != dTl) { firstD = i; dTnewL = dTu; }
@@ -662,7 +832,7 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
                 for (int m = 0; m < U; m++)
                     if (valid_unit(S, m))
                         CoupledSystems_PerBlock_EventFunction<double>(S.sid, S.lane + 32 * m, L.ev_a[m], T, newdt, TD,
-                                                                      L.X[m], L.up[m], S.sPAR, S.gPAR, S.igPAR,
+                                                                      L.X[m], upar_of<U, RHS>(S, L, m), S.sPAR, S.gPAR, S.igPAR,
                                                                       L.ua[m], L.iua[m], S.sACC, S.isACC);
             }
         } else {
@@ -693,7 +863,7 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
             if (i < S.N) {
                 double Tu = Tl, dTu = dTl;
                 int DOu = DOl;
-                CoupledSystems_PerBlock_Finalization<double>(S.sid, i, DOu, Tu, dTu, TD, L.X[m], L.up[m], S.sPAR,
+                CoupledSystems_PerBlock_Finalization<double>(S.sid, i, DOu, Tu, dTu, TD, L.X[m], upar_of<U, RHS>(S, L, m), S.sPAR,
                                                              S.gPAR, S.igPAR, L.ua[m], L.iua[m], S.sACC, S.isACC);
                 if (firstT < 0 && Tu != Tl) { firstT = i; TnewL = Tu; }
                 if (firstD < 0 && dTu != dTl) { firstD = i; dTnewL = dTu; }
@@ -706,8 +876,10 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
 }
 
 /* ---------------------------------------------------------------------------
- * The kernel: warps pull systems from the work counter. */
-template <int U>
+ * The kernel: warps pull systems from the work counter.
+ * RHS = 0: operator W in shared memory (any U); RHS = 1 / 2: operator in
+ * registers (U = 1; 2 = every system of the launch has exactly 32 units). */
+template <int U, int RHS>
 __global__ void __launch_bounds__(128) bes_ensemble_kernel(DeviceProblem P) {
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31;
@@ -722,9 +894,11 @@ __global__ void __launch_bounds__(128) bes_ensemble_kernel(DeviceProblem P) {
     S.vcpt = S.vpt + WarpSmem<U>::NMAX;
     S.vx1 = S.vcpt + WarpSmem<U>::NMAX;
     S.vxu = S.vx1 + WarpSmem<U>::NMAX;
-    S.sPAR = S.vxu + WarpSmem<U>::NMAX;
+    S.vrd = S.vxu + WarpSmem<U>::NMAX;
+    S.sPAR = S.vrd + WarpSmem<U>::NMAX;
     S.sACC = S.sPAR + NSPa;
     S.isACC = reinterpret_cast<int*>(S.sACC + NSAa);
+    S.upsh = S.sPAR + WarpSmem<U>::SYS_DOUBLES;
     S.gPAR = P.gpar;
     S.igPAR = P.igpar;
 
@@ -747,8 +921,12 @@ __global__ void __launch_bounds__(128) bes_ensemble_kernel(DeviceProblem P) {
             const int64_t g = S.off + i;
 #pragma unroll
             for (int c = 0; c < UD; c++) L.X[m][c] = v ? P.state[(int64_t)c * S.tot + g] : 0.0;
+            if constexpr (RHS != 0) {
+                for (int c = 0; c < NUP; c++) S.upsh[i * NUPa + c] = v ? __ldg(P.upar + (int64_t)c * S.tot + g) : 0.0;
+            } else {
 #pragma unroll
-            for (int c = 0; c < NUP; c++) L.up[m][c] = v ? __ldg(P.upar + (int64_t)c * S.tot + g) : 0.0;
+                for (int c = 0; c < NUP; c++) L.up[m][c] = v ? __ldg(P.upar + (int64_t)c * S.tot + g) : 0.0;
+            }
             for (int c = 0; c < NUA; c++) L.ua[m][c] = v ? P.uacc[(int64_t)c * S.tot + g] : 0.0;
 #pragma unroll
             for (int c = 0; c < NIUA; c++) L.iua[m][c] = v ? P.iuacc[(int64_t)c * S.tot + g] : 0;
@@ -757,6 +935,14 @@ __global__ void __launch_bounds__(128) bes_ensemble_kernel(DeviceProblem P) {
         for (int c = lane; c < NSP; c += 32) S.sPAR[c] = P.spar[(int64_t)c * P.n_systems + sid];
         for (int c = lane; c < NSA; c += 32) S.sACC[c] = P.sacc[(int64_t)c * P.n_systems + sid];
         for (int c = lane; c < NISA; c += 32) S.isACC[c] = P.isacc[(int64_t)c * P.n_systems + sid];
+        if constexpr (RHS != 0) {
+            /* stage the system's coupling matrix, zero-padded to 32 x 33 */
+            constexpr int LDC = WarpSmem<1>::LDW;
+            for (int idx = lane; idx < 32 * LDC; idx += 32) {
+                const int r = idx % LDC, c = idx / LDC;
+                S.W[idx] = (r < S.N && c < S.N) ? __ldg(S.C + r + (int64_t)c * S.N) : 0.0;
+            }
+        }
         double TD[2] = {P.time_domain[sid], P.time_domain[P.n_systems + sid]};
         double T = P.actual_time[sid];
         int do_idx = P.ndo > 0 ? P.dense_index[sid] : 0;
@@ -771,7 +957,7 @@ __global__ void __launch_bounds__(128) bes_ensemble_kernel(DeviceProblem P) {
                     for (int c = 0; c < NIUA; c++) L.iua[m][c] = lane + 32 * m < S.N ? P.iuacc_reset[c] : 0;
                 }
             }
-            run_period<U>(S, P, L, cnt, TD, T, do_idx);
+            run_period<U, RHS>(S, P, L, cnt, TD, T, do_idx);
         }
         /* write-back (Solver.cuh:599-648) */
         __syncwarp();

@@ -1,27 +1,44 @@
-/* bes_kernel_u1.cu -- solver kernel instantiation for systems of up to 32 units
+/* bes_kernel_u1.cu -- solver kernel variants for systems of up to 32 units
  * (1 unit(s) per lane). */
 #include "bes_kernel.cuh"
 #include "bes_launch.h"
 
 namespace bes {
 
-template <>
-size_t warp_smem_bytes_t<1>() { return (size_t)WarpSmem<1>::BYTES; }
 
 template <>
-cudaError_t occupancy_t<1>(int warps, int* ctas_per_sm) {
+cudaError_t occupancy_t<1, 1>(int warps, int* ctas_per_sm) {
     const size_t smem = (size_t)warps * WarpSmem<1>::BYTES;
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(bes_ensemble_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(bes_ensemble_kernel<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
         if (e != cudaSuccess) return e;
     }
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, bes_ensemble_kernel<1>, 32 * warps, smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, bes_ensemble_kernel<1, 1>, 32 * warps, smem);
 }
 
 template <>
-cudaError_t launch_t<1>(const DeviceProblem& P, int grid, int warps, cudaStream_t stream) {
+cudaError_t launch_t<1, 1>(const DeviceProblem& P, int grid, int warps, cudaStream_t stream) {
     const size_t smem = (size_t)warps * WarpSmem<1>::BYTES;
-    bes_ensemble_kernel<1><<<grid, 32 * warps, smem, stream>>>(P);
+    bes_ensemble_kernel<1, 1><<<grid, 32 * warps, smem, stream>>>(P);
+    return cudaGetLastError();
+}
+
+template <>
+cudaError_t occupancy_t<1, 2>(int warps, int* ctas_per_sm) {
+    const size_t smem = (size_t)warps * WarpSmem<1>::BYTES;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(bes_ensemble_kernel<1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, bes_ensemble_kernel<1, 2>, 32 * warps, smem);
+}
+
+template <>
+cudaError_t launch_t<1, 2>(const DeviceProblem& P, int grid, int warps, cudaStream_t stream) {
+    const size_t smem = (size_t)warps * WarpSmem<1>::BYTES;
+    bes_ensemble_kernel<1, 2><<<grid, 32 * warps, smem, stream>>>(P);
     return cudaGetLastError();
 }
 

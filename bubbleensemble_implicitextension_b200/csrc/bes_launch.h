@@ -1,5 +1,9 @@
-/* bes_launch.h -- host entry points of the per-class solver kernels
- * (one translation unit per units-per-lane class, so they build in parallel). */
+/* bes_launch.h -- host entry points of the solver kernel variants
+ * (one translation unit per units-per-lane class, so they build in parallel).
+ *
+ * Variant (U, RHS): U units per lane (1, 2, 4 for N <= 32, 64, 128);
+ * RHS 0 keeps the operator in shared memory, RHS 1 keeps it in registers
+ * (U = 1), RHS 2 is RHS 1 for launches whose systems all have 32 units. */
 #ifndef BES_LAUNCH_H
 #define BES_LAUNCH_H
 
@@ -12,16 +16,14 @@ namespace bes {
 
 /* shared-memory bytes one warp of class U needs */
 size_t warp_smem_bytes(int U);
-/* resident CTAs per SM for a CTA of `warps` warps of class U */
-cudaError_t occupancy(int U, int warps, int* ctas_per_sm);
-/* launch the persistent kernel of class U */
-cudaError_t launch(int U, const DeviceProblem& P, int grid, int warps, cudaStream_t stream);
+/* resident CTAs per SM for a CTA of `warps` warps of variant (U, RHS) */
+cudaError_t occupancy(int U, int rhs, int warps, int* ctas_per_sm);
+/* launch the persistent kernel of variant (U, RHS) */
+cudaError_t launch(int U, int rhs, const DeviceProblem& P, int grid, int warps, cudaStream_t stream);
 
-template <int U>
-size_t warp_smem_bytes_t();
-template <int U>
+template <int U, int RHS>
 cudaError_t occupancy_t(int warps, int* ctas_per_sm);
-template <int U>
+template <int U, int RHS>
 cudaError_t launch_t(const DeviceProblem& P, int grid, int warps, cudaStream_t stream);
 
 }  // namespace bes

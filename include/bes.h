@@ -212,7 +212,8 @@ bes_status bes_synchronise_device(bes_solver* h);
 bes_status bes_insert_synchronisation_point(bes_solver* h);
 bes_status bes_synchronise_solver(bes_solver* h);
 
-/* Use the caller's CUDA stream (a cudaStream_t) instead of the solver's own. */
+/* Use the caller's CUDA stream (a cudaStream_t; NULL is the legacy default
+ * stream) instead of the solver's own stream for every later call. */
 bes_status bes_set_stream(bes_solver* h, void* cuda_stream);
 /* device time of the last bes_solve / bes_solve_periods, measured with CUDA
  * events around its launches (valid after bes_synchronise_solver) */
