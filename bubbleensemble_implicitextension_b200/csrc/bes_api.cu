@@ -374,6 +374,20 @@ bes_status bes_device_count(int32_t* count) {
     return BES_OK;
 }
 
+bes_status bes_device_info_get(int32_t device, bes_device_info* out) {
+    if (!out) return BES_ERR_ARGUMENT;
+    std::memset(out, 0, sizeof *out);
+    cudaDeviceProp prop;
+    cudaError_t e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) return fail(nullptr, BES_ERR_CUDA, "cudaGetDeviceProperties(%d): %s", device, cudaGetErrorString(e));
+    std::snprintf(out->name, sizeof out->name, "%s", prop.name);
+    out->cc_major = prop.major;
+    out->cc_minor = prop.minor;
+    out->multiprocessors = prop.multiProcessorCount;
+    out->global_memory_bytes = prop.totalGlobalMem;
+    return BES_OK;
+}
+
 bes_status bes_create(const bes_config* c, bes_solver** out) {
     if (!c || !out) return fail(nullptr, BES_ERR_ARGUMENT, "bes_create: null argument");
     *out = nullptr;

@@ -75,8 +75,12 @@ struct WarpSmem {
     static constexpr int VEC_DOUBLES = 6 * NMAX;
     static constexpr int SYS_DOUBLES = NSPa + NSAa + NISAa; /* ints stored in double slots */
     static constexpr int UP_DOUBLES = NMAX * NUPa;          /* unit parameters, lane-contiguous */
-    static constexpr int DOUBLES = W_DOUBLES + VEC_DOUBLES + SYS_DOUBLES + UP_DOUBLES;
+    /* per-warp stride rounded up to 256 bytes: every warp's vectors stay
+     * 16-byte aligned for the double2 broadcast loads */
+    static constexpr int DOUBLES = (W_DOUBLES + VEC_DOUBLES + SYS_DOUBLES + UP_DOUBLES + 31) / 32 * 32;
     static constexpr int BYTES = DOUBLES * 8;
+    static_assert(DOUBLES % 2 == 0 && W_DOUBLES % 2 == 0 && NMAX % 2 == 0,
+                  "broadcast vectors must start on 16-byte boundaries");
 };
 
 /* halving-tree sum S(L, i) = S(2L, i) + S(2L, i + L), S(P, i) = leaf(i) */

@@ -124,6 +124,11 @@ class ModelInfo(ctypes.Structure):
     ]
 
 
+class DeviceInfo(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 256), ("cc_major", ctypes.c_int32), ("cc_minor", ctypes.c_int32),
+                ("multiprocessors", ctypes.c_int32), ("pad", ctypes.c_int32), ("global_memory_bytes", ctypes.c_uint64)]
+
+
 class CountersStruct(ctypes.Structure):
     _fields_ = [
         ("accepted_steps", ctypes.c_uint64), ("rejected_steps", ctypes.c_uint64),
@@ -172,6 +177,7 @@ SIGNATURES = {
     "bes_load_bubble_sizes": [ctypes.c_char_p, _I32, _DP],
     "bes_load_coupling_matrix": [ctypes.c_char_p, _I32, _DP],
     "bes_device_count": [ctypes.POINTER(ctypes.c_int32)],
+    "bes_device_info_get": [_I32, ctypes.POINTER(DeviceInfo)],
     "bes_measure_fp64_peak": [_I32, ctypes.POINTER(ctypes.c_double)],
     "bes_status_string": [_I32],
     "bes_last_error": [_P],

@@ -233,8 +233,18 @@ bes_status bes_load_bubble_sizes(const char* path, int32_t n, double* out);
  * written to out[row * n + col] */
 bes_status bes_load_coupling_matrix(const char* path, int32_t n, double* out);
 
-/* ListCUDADevices, Interface.cuh:260-311 */
+/* ListCUDADevices, Interface.cuh:260-296 */
 bes_status bes_device_count(int32_t* count);
+
+typedef struct bes_device_info {
+    char name[256];
+    int32_t cc_major, cc_minor;
+    int32_t multiprocessors;
+    int32_t pad;
+    uint64_t global_memory_bytes;
+} bes_device_info;
+/* PrintPropertiesOfSpecificDevice / SelectDeviceByClosestRevision, Interface.cuh:298-346 */
+bes_status bes_device_info_get(int32_t device, bes_device_info* out);
 
 /* Utility, no reference counterpart: the device's FP64 fused multiply-add
  * throughput in TFLOP/s (2 flops per FMA), measured with an FMA loop that

@@ -60,6 +60,39 @@ def _one(v) -> Path:
     return exe
 
 
+DROPIN = [(32, 256, 0), (32, 64, 16)]
+
+
+def dropin_path(ups: int, ns: int, ndo: int = 0) -> Path:
+    return OUT / f"dropin_n{ups}_s{ns}_d{ndo}"
+
+
+def build_dropin() -> list[Path]:
+    """The same driver (ref_harness.cu) compiled against include/dropin/, i.e.
+    the C++ ProblemSolver shim over libbes.so instead of the reference headers.
+    Needs no reference tree."""
+    OUT.mkdir(exist_ok=True)
+    root = HERE.parent
+    pkg = root / "bubbleensemble_implicitextension_b200"
+    src = HERE / "ref_harness.cu"
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    outs = []
+    for ups, ns, ndo in DROPIN:
+        exe = dropin_path(ups, ns, ndo)
+        deps = [src, root / "include" / "bes_problem_solver.h", root / "include" / "bes.h", pkg / "libbes.so"]
+        if exe.exists() and all(exe.stat().st_mtime > d.stat().st_mtime for d in deps if d.exists()):
+            outs.append(exe)
+            continue
+        cmd = [nvcc, "-O2", "--std=c++17", "-w", f"-DHARNESS_UPS={ups}", f"-DHARNESS_NS={ns}", f"-DHARNESS_NDO={ndo}",
+               "-I", str(root / "include" / "dropin"), "-I", str(root / "include"), str(src), "-o", str(exe),
+               "-L", str(pkg), "-lbes", "-Xlinker", "-rpath=$ORIGIN/../../bubbleensemble_implicitextension_b200"]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"drop-in build failed ({exe.name}):\n{res.stderr[-4000:]}")
+        outs.append(exe)
+    return outs
+
+
 def build() -> list[Path]:
     """Build every variant (no-op when the reference tree is absent)."""
     if not available():
