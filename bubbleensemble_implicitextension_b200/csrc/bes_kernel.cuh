@@ -26,9 +26,10 @@
  * registers, so a step needs no block barrier at all.
  *
  * Arithmetic order (identical in the CPU oracle): sums over units are the
- * halving tree over units padded with zeros to 32U; the row products
- * accumulate columns 0..N-1 with fma; every fused multiply-add is explicit
- * (the file is compiled with --fmad=false).
+ * halving tree over units padded with zeros to 32U; the row products use
+ * four interleaved fma chains over the columns (j mod 4) combined as
+ * (s0 + s1) + (s2 + s3); every fused multiply-add is explicit (the file is
+ * compiled with --fmad=false).
  */
 #ifndef BES_KERNEL_CUH
 #define BES_KERNEL_CUH
@@ -128,6 +129,29 @@ __device__ __forceinline__ double warp_tree_max(const double (&v)[U]) {
     return s;
 }
 
+/* max of a and halving-tree sum of b in one interleaved butterfly */
+template <int U>
+__device__ __forceinline__ void warp_tree_max_sum(const double (&a)[U], const double (&b)[U], double& amax,
+                                                  double& bsum) {
+    double x[U], y[U];
+#pragma unroll
+    for (int m = 0; m < U; m++) { x[m] = a[m]; y[m] = b[m]; }
+#pragma unroll
+    for (int h = U / 2; h >= 1; h /= 2)
+#pragma unroll
+        for (int m = 0; m < h; m++) { x[m] = fmax(x[m], x[m + h]); y[m] = y[m] + y[m + h]; }
+    double s = x[0], t = y[0];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        const double so = __shfl_xor_sync(FULL, s, o);
+        const double to = __shfl_xor_sync(FULL, t, o);
+        s = fmax(s, so);
+        t = t + to;
+    }
+    amax = s;
+    bsum = t;
+}
+
 __device__ __forceinline__ double warp_min(double s) {
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) s = fmin(s, __shfl_xor_sync(FULL, s, o));
@@ -205,19 +229,30 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U>& S, const DeviceProblem&
     for (int m = 0; m < U; m++) {
         const int i = S.lane + 32 * m;
         if (i < N) {
-            double b = 0.0, ax = 0.0;
+            double b0 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0, a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
             const double* Ci = S.C + i;
             double* Wi = S.W + i;
-#pragma unroll 8
-            for (int j = 0; j < N; j++) {
-                double cij = __ldg(Ci + (int64_t)j * N);
-                double x1 = S.vx1[j];
-                b = fma(cij, S.vcpt[j], b);
-                ax = fma(cij * x1, S.vxu[j], ax);
-                Wi[j * LDW] = (rd[m] * cij) * x1;
+            const double rdm = rd[m];
+            /* one column: chain k of the four interleaved chains */
+            auto col = [&](int j, double& bk, double& ak) {
+                const double cij = __ldg(Ci + (int64_t)j * N);
+                const double x1 = S.vx1[j];
+                bk = fma(cij, S.vcpt[j], bk);
+                ak = fma(cij * x1, S.vxu[j], ak);
+                Wi[j * LDW] = (rdm * cij) * x1;
+            };
+            int j = 0;
+            for (; j + 3 < N; j += 4) {
+                col(j, b0, a0);
+                col(j + 1, b1, a1);
+                col(j + 2, b2, a2);
+                col(j + 3, b3, a3);
             }
-            b = fma(rd[m], b, xu[m]);
-            ax = fma(rd[m], ax, xu[m]);
+            if (j < N) col(j, b0, a0);
+            if (j + 1 < N) col(j + 1, b1, a1);
+            if (j + 2 < N) col(j + 2, b2, a2);
+            double b = fma(rdm, (b0 + b1) + (b2 + b3), xu[m]);
+            double ax = fma(rdm, (a0 + a1) + (a2 + a3), xu[m]);
             r[m] = b - ax;
         } else {
             r[m] = 0.0;
@@ -260,11 +295,19 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U>& S, const DeviceProblem&
         for (int m = 0; m < U; m++) {
             const int i = S.lane + 32 * m;
             if (i < N) {
-                double qi = p[m];
+                double q0 = 0.0, q1 = 0.0, q2 = 0.0, q3 = 0.0;
                 const double* Wi = S.W + i;
-#pragma unroll 8
-                for (int j = 0; j < N; j++) qi = fma(Wi[j * LDW], S.vp[j], qi);
-                q[m] = qi;
+                int j = 0;
+                for (; j + 3 < N; j += 4) {
+                    q0 = fma(Wi[j * LDW], S.vp[j], q0);
+                    q1 = fma(Wi[(j + 1) * LDW], S.vp[j + 1], q1);
+                    q2 = fma(Wi[(j + 2) * LDW], S.vp[j + 2], q2);
+                    q3 = fma(Wi[(j + 3) * LDW], S.vp[j + 3], q3);
+                }
+                if (j < N) q0 = fma(Wi[j * LDW], S.vp[j], q0);
+                if (j + 1 < N) q1 = fma(Wi[(j + 1) * LDW], S.vp[j + 1], q1);
+                if (j + 2 < N) q2 = fma(Wi[(j + 2) * LDW], S.vp[j + 2], q2);
+                q[m] = p[m] + ((q0 + q1) + (q2 + q3));
                 const double* Wc = S.W + (int64_t)i * LDW;
                 const double* vpt = S.vpt;
                 auto leaf = [&](int j) -> double { return j < N ? Wc[j] * vpt[j] : 0.0; };
@@ -285,13 +328,14 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U>& S, const DeviceProblem&
             rt[m] = fma(-alpha, qt[m], rt[m]);
             ar[m] = fabs(r[m]);
         }
-        double rmax = warp_tree_max<U>(ar);
+#pragma unroll
+        for (int m = 0; m < U; m++) prod[m] = r[m] * rt[m];
+        double rmax, rho_next;
+        warp_tree_max_sum<U>(ar, prod, rmax, rho_next);
         rho2 = rho1;
         done++;
         if (rmax < 1e-6) { exited = true; break; }
-#pragma unroll
-        for (int m = 0; m < U; m++) prod[m] = r[m] * rt[m];
-        rho1 = warp_tree_sum<U>(prod);
+        rho1 = rho_next;
     }
     if (!exited) capped = true;
 #pragma unroll
@@ -337,7 +381,7 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
     S.vrd[i] = rd;
     __syncwarp();
     double wr[32], wc[32];
-    double b = 0.0, ax = 0.0;
+    double bs[4] = {0.0, 0.0, 0.0, 0.0}, as[4] = {0.0, 0.0, 0.0, 0.0};
     const double* Crow = S.W + i;        /* C[i][j] at i + j*LDC */
     const double* Ccol = S.W + i * LDC;  /* C[j][i] at j + i*LDC */
 #pragma unroll
@@ -347,16 +391,16 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
         const double x1j = S.vx1[j];
         const bool in = NFIX != 0 || j < N;
         if (in) {
-            b = fma(cij, S.vcpt[j], b);
-            ax = fma(cij * x1j, S.vxu[j], ax);
+            bs[j & 3] = fma(cij, S.vcpt[j], bs[j & 3]);
+            as[j & 3] = fma(cij * x1j, S.vxu[j], as[j & 3]);
         }
         wr[j] = in ? (rd * cij) * x1j : 0.0;
         wc[j] = in ? (S.vrd[j] * cji) * x1 : 0.0;
     }
     double r = 0.0;
     if (valid) {
-        b = fma(rd, b, xu);
-        ax = fma(rd, ax, xu);
+        const double b = fma(rd, (bs[0] + bs[1]) + (bs[2] + bs[3]), xu);
+        const double ax = fma(rd, (as[0] + as[1]) + (as[2] + as[3]), xu);
         r = b - ax;
     }
     double rt = r, x = xu, p = 0.0, pt = 0.0;
@@ -381,13 +425,14 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
         S.vp[i] = p;
         S.vpt[i] = pt;
         __syncwarp();
-        double q = p;
+        double qs[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
         for (int j = 0; j < 32; j += 2) {
             const double2 a = vp2[j / 2];
-            if (NFIX != 0 || j < N) q = fma(wr[j], a.x, q);
-            if (NFIX != 0 || j + 1 < N) q = fma(wr[j + 1], a.y, q);
+            if (NFIX != 0 || j < N) qs[j & 3] = fma(wr[j], a.x, qs[j & 3]);
+            if (NFIX != 0 || j + 1 < N) qs[(j + 1) & 3] = fma(wr[j + 1], a.y, qs[(j + 1) & 3]);
         }
+        double q = p + ((qs[0] + qs[1]) + (qs[2] + qs[3]));
         /* first tree level t_k + t_{k+16} on the loads, then the halving tree over 16 */
         double u[16];
 #pragma unroll
@@ -405,12 +450,13 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
         r = fma(-alpha, q, r);
         rt = fma(-alpha, qt, rt);
         double ar[1] = {fabs(r)};
-        const double rmax = warp_tree_max<1>(ar);
+        prod[0] = r * rt;
+        double rmax, rho_next;
+        warp_tree_max_sum<1>(ar, prod, rmax, rho_next);
         rho2 = rho1;
         done++;
         if (rmax < 1e-6) { exited = true; break; }
-        prod[0] = r * rt;
-        rho1 = warp_tree_sum<1>(prod);
+        rho1 = rho_next;
     }
     if (!exited) capped = true;
     F[0][IC] = x;

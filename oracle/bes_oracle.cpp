@@ -12,9 +12,11 @@
  *     for N >= 32 this is exactly the reference's order, for N < 32 it is the
  *     correct sum (the reference's reduction is wrong there: it returns
  *     2*s[0] because nP2Warps = 0);
- *   - the direct products (coupling value, A*x0, A*p) accumulate columns
- *     0..N-1 sequentially with fma, as Steppers.cuh:576-584, :647-666 and
- *     :683-688 do;
+ *   - the direct products (coupling value, A*x0, A*p; Steppers.cuh:576-584,
+ *     :647-666, :683-688, which accumulate columns 0..N-1 in one chain)
+ *     use four interleaved fma chains over the columns j = 0, 1, 2, 3 mod 4,
+ *     combined as (s0 + s1) + (s2 + s3) (a shorter dependency chain on the
+ *     GPU); A*p adds that sum to p_i;
  *   - the operator element is W_ij = (rD_i * C_ij) * X1sq_j (Steppers.cuh:685).
  * The product kernel follows the same order, so oracle and kernel agree
  * bit for bit.
@@ -76,6 +78,14 @@ inline void km_ode(double X0, double X1, double T, const double* u,
     *CPF = rD;
 }
 
+/* four interleaved fma chains over the columns, combined as (s0 + s1) + (s2 + s3) */
+template <class A, class B>
+inline double row_sum4(int n, A a, B b) {
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int j = 0; j < n; j++) s[j & 3] = fma(a(j), b(j), s[j & 3]);
+    return (s[0] + s[1]) + (s[2] + s[3]);
+}
+
 inline int next_pow2_32(int n) {
     int p = 32;
     while (p < n) p *= 2;
@@ -128,11 +138,9 @@ int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
     }
     /* b = rD (C CPT) + x_u ; r = b - A x_u  (Steppers.cuh:495-505, :576-584, :647-666) */
     for (int i = 0; i < N; i++) {
-        double bi = 0.0;
-        for (int j = 0; j < N; j++) bi = fma(C[i + (long)j * N], w.cpt[j], bi);
+        double bi = row_sum4(N, [&](int j) { return C[i + (long)j * N]; }, [&](int j) { return w.cpt[j]; });
         bi = fma(w.rd[i], bi, w.xu[i]);
-        double ax = 0.0;
-        for (int j = 0; j < N; j++) ax = fma(C[i + (long)j * N] * w.x1sq[j], w.xu[j], ax);
+        double ax = row_sum4(N, [&](int j) { return C[i + (long)j * N] * w.x1sq[j]; }, [&](int j) { return w.xu[j]; });
         ax = fma(w.rd[i], ax, w.xu[i]);
         w.r[i] = bi - ax;
         w.rt[i] = w.r[i];
@@ -157,9 +165,7 @@ int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
         }
         /* q = A p (row sums) and qt = A^T pt (tree sums), Steppers.cuh:669-706 */
         for (int i = 0; i < N; i++) {
-            double qi = w.p[i];
-            for (int j = 0; j < N; j++) qi = fma(w.W[i + (long)j * N], w.p[j], qi);
-            w.q[i] = qi;
+            w.q[i] = w.p[i] + row_sum4(N, [&](int j) { return w.W[i + (long)j * N]; }, [&](int j) { return w.p[j]; });
             for (int j = 0; j < N; j++) w.tmp2[j] = w.W[j + (long)i * N] * w.pt[j];
             w.qt[i] = w.pt[i] + tree_sum(w.tmp2.data(), N, w.tmp.data());
         }
