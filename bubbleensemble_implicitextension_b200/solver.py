@@ -137,6 +137,28 @@ class CountersStruct(ctypes.Structure):
     ]
 
 
+class NoallocProblem(ctypes.Structure):
+    """bes_noalloc_problem (include/bes.h): device pointers of a caller-owned ensemble."""
+    _P64 = ctypes.c_void_p
+    _fields_ = [
+        ("n_systems", ctypes.c_int32), ("algorithm", ctypes.c_int32), ("total_units", ctypes.c_int64),
+        ("units_host", ctypes.POINTER(ctypes.c_int32)),
+        ("units", _P64), ("unit_offset", _P64), ("coupling_offset", _P64), ("coupling", _P64),
+        ("state", _P64), ("upar", _P64), ("uacc", _P64), ("iuacc", _P64),
+        ("spar", _P64), ("sacc", _P64), ("isacc", _P64), ("gpar", _P64), ("igpar", _P64),
+        ("time_domain", _P64), ("actual_time", _P64), ("rtol", _P64), ("atol", _P64),
+        ("event_tol", _P64), ("event_dir", _P64), ("uacc_reset", _P64), ("iuacc_reset", _P64),
+        ("dense_time", _P64), ("dense_state", _P64), ("dense_index", _P64),
+        ("n_accepted", _P64), ("n_rejected", _P64), ("n_bicg_iter", _P64), ("n_rhs", _P64), ("status", _P64),
+        ("dt0", ctypes.c_double), ("dtmin", ctypes.c_double), ("dtmax", ctypes.c_double),
+        ("grow", ctypes.c_double), ("shrink", ctypes.c_double), ("do_min_dt", ctypes.c_double),
+        ("ndo", ctypes.c_int32), ("do_save_frequency", ctypes.c_int32),
+        ("bicg_max_iter", ctypes.c_int32), ("warps_per_block", ctypes.c_int32),
+        ("max_steps_per_period", ctypes.c_int64),
+        ("error_message", ctypes.c_char_p), ("error_capacity", ctypes.c_int32), ("pad", ctypes.c_int32),
+    ]
+
+
 # every exported symbol of include/bes.h with its argument types
 _I32, _D, _P = ctypes.c_int32, ctypes.c_double, ctypes.c_void_p
 _DP = ctypes.POINTER(ctypes.c_double)
@@ -179,6 +201,7 @@ SIGNATURES = {
     "bes_device_count": [ctypes.POINTER(ctypes.c_int32)],
     "bes_device_info_get": [_I32, ctypes.POINTER(DeviceInfo)],
     "bes_measure_fp64_peak": [_I32, ctypes.POINTER(ctypes.c_double)],
+    "bes_solve_periods_noalloc": [ctypes.POINTER(NoallocProblem), _I32, _I32, _P],
     "bes_status_string": [_I32],
     "bes_last_error": [_P],
 }

@@ -252,6 +252,73 @@ bes_status bes_device_info_get(int32_t device, bes_device_info* out);
  * denominator of the FP64 solver kernel. */
 bes_status bes_measure_fp64_peak(int32_t device, double* tflops);
 
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory: an application that already owns the GPU's memory (a framework that
+ * reserves the device and hands out slices of its own pool, or a real-time
+ * loop in which cudaMalloc could block or synchronise) lays out every input
+ * and output in memory it holds and passes device pointers here; the call
+ * allocates nothing (no cudaMalloc, no cudaFree, no host allocation).
+ * Arrays use the layout of bes_get_array / bes_set_array for the compiled
+ * system definition (bes_model_info_get).  The solver's scratch (per-class
+ * work counters and the processing order) is a fixed device array inside the
+ * library, held by every GPU that loads it until exit: at most
+ * BES_NOALLOC_MAX_SYSTEMS systems per call; larger ensembles are rejected
+ * with BES_ERR_ARGUMENT.  The first call on a device (with that device
+ * current) looks up the scratch's device address; make that first call before
+ * any stream capture.  Every call resets the scratch before its launches, and
+ * all calls share it: calls that overlap on the GPU race and must be
+ * serialised by the caller.  Runs asynchronously on `stream` (NULL: the
+ * legacy default stream) and integrates n_periods periods of systems
+ * [0, n_systems), resetting accessories before period reset_at, like
+ * bes_solve_periods. */
+#define BES_NOALLOC_MAX_SYSTEMS 65536
+typedef struct bes_noalloc_problem {
+    int32_t n_systems;
+    int32_t algorithm;                 /* BES_RK4 or BES_RKCK45 */
+    int64_t total_units;
+    const int32_t* units_host;         /* host copy of the unit counts [n_systems] (launch planning) */
+    /* device arrays */
+    const int32_t* units;              /* [n_systems] */
+    const int64_t* unit_offset;        /* [n_systems] */
+    const int64_t* coupling_offset;    /* [n_systems], in doubles */
+    const double* coupling;            /* N x N column-major matrices */
+    double* state;                     /* [UD][total_units] */
+    const double* upar;                /* [NUP][total_units] */
+    double* uacc;                      /* [NUA][total_units] */
+    int32_t* iuacc;                    /* [NiUA][total_units] */
+    double* spar;                      /* [NSP][n_systems] (may be NULL when NSP = 0) */
+    double* sacc;                      /* [NSA][n_systems] */
+    int32_t* isacc;                    /* [NiSA][n_systems] */
+    double* gpar;                      /* [NGP] */
+    int32_t* igpar;                    /* [NiGP] */
+    double* time_domain;               /* [2][n_systems] */
+    double* actual_time;               /* [n_systems] */
+    const double* rtol;                /* [UD][n_systems] */
+    const double* atol;                /* [UD][n_systems] */
+    const double* event_tol;           /* [NE] */
+    const int32_t* event_dir;          /* [NE] */
+    const double* uacc_reset;          /* [NUA] */
+    const int32_t* iuacc_reset;        /* [NiUA] */
+    double* dense_time;                /* [ndo][n_systems] (NULL when ndo = 0) */
+    double* dense_state;               /* [ndo][UD][total_units] */
+    int32_t* dense_index;              /* [n_systems] */
+    uint64_t* n_accepted;              /* [n_systems] counters, accumulated */
+    uint64_t* n_rejected;
+    uint64_t* n_bicg_iter;
+    uint64_t* n_rhs;
+    int32_t* status;                   /* [n_systems], OR of BES_STATUS_* */
+    /* options (defaults of SolverOption where 0) */
+    double dt0, dtmin, dtmax, grow, shrink, do_min_dt;
+    int32_t ndo, do_save_frequency;
+    int32_t bicg_max_iter, warps_per_block;
+    int64_t max_steps_per_period;
+    char* error_message;               /* optional caller buffer for a message on failure */
+    int32_t error_capacity;
+    int32_t pad;
+} bes_noalloc_problem;
+bes_status bes_solve_periods_noalloc(const bes_noalloc_problem* problem, int32_t n_periods, int32_t reset_at,
+                                     void* stream);
+
 const char* bes_status_string(bes_status status);
 const char* bes_last_error(const bes_solver* h);
 
