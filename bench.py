@@ -51,6 +51,26 @@ WORKLOAD = ("c1_period1: 256 systems (16 amplitudes 0.5-2 bar x 16 frequencies 2
             "acoustic period of every system from rest")
 DATA = "synthetic: seeded PCG64 radii, reference parameter formulas (CollapseStrength.cu:329-357)"
 
+WORKLOADS = {
+    "c1_period1": WORKLOAD,
+    "c2_period1": ("c2_period1: 16384 systems with N drawn from {4,8,16,32,48,64} (seed 2), one random 3-D cloud per "
+                   "system in a 500 um sphere (min separation 20 um), R_E ~ U(1,10) um, dual-frequency drive "
+                   "f2 = k f1 (f1 U(20,100) kHz, k in {2,3}, amplitudes U(0,1.5) bar), rtol = atol alternating "
+                   "1e-8 / 1e-10, one launch plan for all sizes; one step = one acoustic period of every system from rest"),
+    "c3_period1": ("c3_period1: 4096 systems sharing one N = 128 cloud (1 mm cube, R_E lognormal median 4 um sigma 0.4 "
+                   "clipped to [1,12] um, seed 3), 200 kHz at 1.2 bar, initial radii perturbed by 1e-3 U(-1,1) per "
+                   "bubble, RKCK45 rtol=atol=1e-10, FP64 BiCG; one step = one acoustic period of every system from rest"),
+}
+
+
+def make_ensemble(name):
+    from bubbleensemble_implicitextension_b200 import workloads as W
+    if name == "c1_period1":
+        return W.c1_ensemble(n_periods=1, reset_at=-1)
+    if name == "c2_period1":
+        return W.c2_ensemble(n_periods=1, reset_at=-1)
+    return W.c3_ensemble(n_periods=1, reset_at=-1)
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -58,6 +78,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=list(WORKLOADS), default="c1_period1",
+                    help="c1_period1 (default, the headline), c2_period1, c3_period1")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-systems", type=int, default=32)
     ap.add_argument("--systems", type=int, default=256,
@@ -172,8 +194,8 @@ def cpu_baseline(ens, n_sample):
     O.run(ens, n_periods=1, reset_at=-1, systems=systems, threads=threads)
     dt = time.perf_counter() - t0
     return {"value": len(systems) / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"CPU oracle (C++ FP64, OpenMP {threads} threads): period 1 of {len(systems)} of the 256 "
-                      f"systems (every {ens.n_systems // len(systems)}th), {dt:.1f} s"}
+            "sample": f"CPU oracle (C++ FP64, OpenMP {threads} threads): period 1 of {len(systems)} of the "
+                      f"{ens.n_systems} systems (every {ens.n_systems // len(systems)}th), {dt:.1f} s"}
 
 
 def run_b200(args, rank, world, local):
@@ -185,7 +207,7 @@ def run_b200(args, rank, world, local):
     V = S.ListOfVariables
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    ens = W.c1_ensemble(n_periods=1, reset_at=-1)
+    ens = make_ensemble(args.workload)
     if args.systems < ens.n_systems:
         ens = ens.subset(list(range(0, ens.n_systems, ens.n_systems // args.systems))[:args.systems])
     ens.max_steps_per_period = 1_000_000
@@ -279,14 +301,17 @@ def run_b200(args, rank, world, local):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": DATA,
-        "config": {"workload": WORKLOAD, "systems": ens.n_systems, "units_per_system": 32,
+        "config": {"workload": WORKLOADS[args.workload], "systems": ens.n_systems,
+                   "units_per_system": int(ens.units[0]) if len(set(ens.units.tolist())) == 1 else "mixed",
+                   "total_units": ens.total_units,
                    "periods_per_step": 1, "l2": "flushed between timed steps (256 MiB write, untimed)",
                    "parallelism": f"{world} independent ensemble replica(s), one per GPU"},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak if peak else None, "traffic": read_traffic(),
+                     "frac": achieved / peak if peak else None,
+                     "traffic": read_traffic() if args.workload == "c1_period1" else None,
                      "peak_source": "measured live: bes_measure_fp64_peak FMA-throughput loop (no FP64 figure in "
                                     "MEASURED_PEAKS.json)",
-                     "flops_per_launch": flops, "kernel": "bes::bes_ensemble_kernel<1>"},
+                     "flops_per_launch": flops, "kernel": "bes::bes_ensemble_kernel (all classes of the launch plan)"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(in_bytes),
                 "d2h_bytes_per_step": int(out_bytes)},
         "gpu_launches": launches,
@@ -302,6 +327,11 @@ def run_b200(args, rank, world, local):
 def run_reference(args, rank, world):
     if rank != 0:
         return None
+    if args.workload == "c2_period1":
+        return {"impl": "reference", "unavailable": "the reference solver takes one unit count (template UPS) and one "
+                "global coupling matrix; c2_period1 has per-system sizes and geometries"}
+    if args.workload == "c3_period1":
+        return {"impl": "reference", "unavailable": "no reference harness built for 4096 systems x 128 units"}
     from bubbleensemble_implicitextension_b200 import workloads as W
     from oracle import build_ref, ref_io
 

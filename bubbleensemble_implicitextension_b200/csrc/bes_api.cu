@@ -93,6 +93,14 @@ struct bes_solver {
     int class_begin[3] = {0, 0, 0}, class_count[3] = {0, 0, 0};
     bool class0_all32 = false;
     int sm_count = 148;
+    /* the classes run concurrently: fork/join streams, and the whole solve is
+     * captured once into a CUDA graph that later calls replay */
+    cudaStream_t class_stream[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t fork_ev = nullptr, join_ev[3] = {nullptr, nullptr, nullptr};
+    cudaGraphExec_t gexec = nullptr;
+    int g_periods = -1, g_reset = -2, g_launches = 0;
+    bool graph_dirty = true;
+    int use_graph = 1;
     float last_ms = 0.f;
     int last_launches = 0;
     std::string err;
@@ -210,6 +218,12 @@ void free_all(bes_solver* h) {
     for (void* p : dev)
         if (p) cudaFree(p);
     if (h->h_order) cudaFreeHost(h->h_order);
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    for (int c = 0; c < 3; c++) {
+        if (h->class_stream[c]) cudaStreamDestroy(h->class_stream[c]);
+        if (h->join_ev[c]) cudaEventDestroy(h->join_ev[c]);
+    }
+    if (h->fork_ev) cudaEventDestroy(h->fork_ev);
     if (h->sync_event) cudaEventDestroy(h->sync_event);
     if (h->t0) cudaEventDestroy(h->t0);
     if (h->t1) cudaEventDestroy(h->t1);
@@ -240,6 +254,7 @@ bes_status build_order(bes_solver* h) {
     if (nact > 0)
         CUDA_TRY(h, cudaMemcpyAsync(h->d_order, h->h_order, sizeof(int32_t) * nact, cudaMemcpyHostToDevice, h->stream));
     h->order_dirty = false;
+    h->graph_dirty = true;
     return BES_OK;
 }
 
@@ -291,15 +306,16 @@ DeviceProblem make_problem(bes_solver* h) {
     return P;
 }
 
-bes_status launch_class(bes_solver* h, DeviceProblem P, int cls) {
+struct ClassLaunch {
+    int U, rhs, grid, wpb;
+};
+
+/* launch shape of one class (no stream work: safe before a capture) */
+bes_status plan_class(bes_solver* h, int cls, ClassLaunch* L) {
     const int U = cls == 0 ? 1 : (cls == 1 ? 2 : 4);
     /* N <= 32: operator in registers (2: every system has exactly 32 units) */
     const int rhs = cls == 0 ? (h->class0_all32 ? 2 : 1) : 0;
     const int count = h->class_count[cls];
-    if (count == 0) return BES_OK;
-    P.order = h->d_order + h->class_begin[cls];
-    P.n_active = count;
-    P.work_counter = h->d_work + cls;
     const int smem_warp = (int)bes::warp_smem_bytes(U);
     int wpb = h->warps_per_block;
     if (wpb <= 0) {
@@ -313,9 +329,32 @@ bes_status launch_class(bes_solver* h, DeviceProblem P, int cls) {
     if (per_sm < 1)
         return fail(h, BES_ERR_CUDA, "solver kernel (U=%d) cannot be resident with %d warps per block", U, wpb);
     const int needed = (count + wpb - 1) / wpb;
-    const int grid = std::max(1, std::min(needed, per_sm * h->sm_count));
-    CUDA_TRY(h, bes::launch(U, rhs, P, grid, wpb, h->stream));
-    h->last_launches++;
+    L->U = U;
+    L->rhs = rhs;
+    L->wpb = wpb;
+    L->grid = std::max(1, std::min(needed, per_sm * h->sm_count));
+    return BES_OK;
+}
+
+/* the whole solve on stream s: reset the work counters, fork one stream per
+ * non-empty class, join back into s */
+bes_status enqueue_solve(bes_solver* h, DeviceProblem P, cudaStream_t s, const ClassLaunch* L, int* launches) {
+    *launches = 0;
+    CUDA_TRY(h, cudaMemsetAsync(h->d_work, 0, sizeof(int32_t) * 4, s));
+    CUDA_TRY(h, cudaEventRecord(h->fork_ev, s));
+    for (int cls = 0; cls < 3; cls++) {
+        if (h->class_count[cls] == 0) continue;
+        DeviceProblem Pc = P;
+        Pc.order = h->d_order + h->class_begin[cls];
+        Pc.n_active = h->class_count[cls];
+        Pc.work_counter = h->d_work + cls;
+        cudaStream_t cs = h->class_stream[cls];
+        CUDA_TRY(h, cudaStreamWaitEvent(cs, h->fork_ev, 0));
+        CUDA_TRY(h, bes::launch(L[cls].U, L[cls].rhs, Pc, L[cls].grid, L[cls].wpb, cs));
+        CUDA_TRY(h, cudaEventRecord(h->join_ev[cls], cs));
+        CUDA_TRY(h, cudaStreamWaitEvent(s, h->join_ev[cls], 0));
+        (*launches)++;
+    }
     return BES_OK;
 }
 
@@ -516,6 +555,11 @@ bes_status bes_create(const bes_config* c, bes_solver** out) {
     CREATE_TRY(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
     h->stream = h->own_stream;
     CREATE_TRY(cudaEventCreateWithFlags(&h->sync_event, cudaEventDisableTiming));
+    CREATE_TRY(cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming));
+    for (int c = 0; c < 3; c++) {
+        CREATE_TRY(cudaStreamCreateWithFlags(&h->class_stream[c], cudaStreamNonBlocking));
+        CREATE_TRY(cudaEventCreateWithFlags(&h->join_ev[c], cudaEventDisableTiming));
+    }
     CREATE_TRY(cudaEventCreate(&h->t0));
     CREATE_TRY(cudaEventCreate(&h->t1));
     for (auto& b : h->buf) {
@@ -596,9 +640,11 @@ bes_status bes_solver_option(bes_solver* h, int32_t option, double value) {
             h->bicg_max_iter = (int)value;
             break;
         case BES_OPT_WARPS_PER_BLOCK: h->warps_per_block = (int)value; break;
+        case BES_OPT_USE_CUDA_GRAPH: h->use_graph = value != 0.0; break;
         default:
             return fail(h, BES_ERR_OPTION, "SolverOption: option %d needs an index argument or is not applicable", option);
     }
+    h->graph_dirty = true; /* the kernel arguments carry the options */
     return BES_OK;
 }
 
@@ -921,12 +967,38 @@ bes_status bes_solve_periods(bes_solver* h, int32_t n_periods, int32_t reset_at)
     DeviceProblem P = make_problem(h);
     P.n_periods = n_periods;
     P.reset_at = reset_at;
-    h->last_launches = 0;
-    CUDA_TRY(h, cudaMemsetAsync(h->d_work, 0, sizeof(int32_t) * 4, h->stream));
-    CUDA_TRY(h, cudaEventRecord(h->t0, h->stream));
+    ClassLaunch L[3] = {};
     for (int cls = 0; cls < 3; cls++)
-        if ((st = launch_class(h, P, cls))) return st;
+        if (h->class_count[cls] > 0 && (st = plan_class(h, cls, &L[cls]))) return st;
+    if (!h->use_graph) {
+        CUDA_TRY(h, cudaEventRecord(h->t0, h->stream));
+        if ((st = enqueue_solve(h, P, h->stream, L, &h->last_launches))) return st;
+        CUDA_TRY(h, cudaEventRecord(h->t1, h->stream));
+        return BES_OK;
+    }
+    if (h->graph_dirty || h->gexec == nullptr || h->g_periods != n_periods || h->g_reset != reset_at) {
+        /* capture on the solver's own stream; the graph is replayed on the caller's */
+        if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+        CUDA_TRY(h, cudaStreamSynchronize(h->own_stream));
+        CUDA_TRY(h, cudaStreamBeginCapture(h->own_stream, cudaStreamCaptureModeThreadLocal));
+        int launches = 0;
+        st = enqueue_solve(h, P, h->own_stream, L, &launches);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(h->own_stream, &graph);
+        if (st) { if (graph) cudaGraphDestroy(graph); return st; }
+        if (e != cudaSuccess) return fail(h, BES_ERR_CUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&h->gexec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return fail(h, BES_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+        h->g_periods = n_periods;
+        h->g_reset = reset_at;
+        h->g_launches = launches;
+        h->graph_dirty = false;
+    }
+    CUDA_TRY(h, cudaEventRecord(h->t0, h->stream));
+    CUDA_TRY(h, cudaGraphLaunch(h->gexec, h->stream));
     CUDA_TRY(h, cudaEventRecord(h->t1, h->stream));
+    h->last_launches = h->g_launches;
     return BES_OK;
 }
 

@@ -68,6 +68,7 @@ class ListOfSolverOptions(IntEnum):
     MaxStepsPerPeriod = 100
     BiCGMaxIterations = 101
     WarpsPerBlock = 102
+    UseCudaGraph = 103
 
 
 class Algorithms(IntEnum):

@@ -252,39 +252,61 @@ def c1_ensemble(n_pa: int = 16, n_f: int = 16, n_units: int = 32, spacing_um: fl
                                                      "positions_um": pos, "cstr": cstr})
 
 
+def _ball_points(rng, count: int, radius: float) -> np.ndarray:
+    """`count` points uniform in a ball (rejection from the enclosing cube)."""
+    out = np.empty((0, 3))
+    while len(out) < count:
+        cand = rng.uniform(-radius, radius, (2 * (count - len(out)) + 16, 3))
+        out = np.concatenate([out, cand[(cand ** 2).sum(1) <= radius * radius]])
+    return out[:count]
+
+
 def c2_ensemble(n_systems: int = 16384, seed: int = 2, n_periods: int = 64, reset_at: int = 32,
                 sizes=(4, 8, 16, 32, 48, 64), sphere_um: float = 500.0, min_sep_um: float = 20.0) -> Ensemble:
-    """Uneven ensemble: N from `sizes`, random 3-D clouds in a sphere with a
-    minimum separation, radii U(1, 10) um, dual-frequency drive f2 = k f1
-    (k in {2, 3}), amplitudes U(0, 1.5) bar, tolerances 1e-8 / 1e-10 alternating."""
+    """Uneven ensemble: N from `sizes`, one random 3-D cloud per system (uniform
+    in a sphere, points closer than `min_sep_um` redrawn), radii U(1, 10) um,
+    dual-frequency drive f2 = k f1 (f1 U(20, 100) kHz, k in {2, 3}), amplitudes
+    U(0, 1.5) bar each, tolerances 1e-8 / 1e-10 alternating by system."""
     rng = np.random.default_rng(seed)
     units = rng.choice(np.asarray(sizes), n_systems).astype(np.int32)
-    ups, coups, states = [], [], []
-    rtol = np.empty((2, n_systems))
-    for s in range(n_systems):
-        n = int(units[s])
-        pts = []
-        while len(pts) < n:
-            p = rng.uniform(-sphere_um, sphere_um, 3)
-            if p @ p > sphere_um ** 2:
-                continue
-            if all(np.linalg.norm(p - q) >= min_sep_um for q in pts):
-                pts.append(p)
-        pts = np.asarray(pts)
-        r = rng.uniform(1.0, 10.0, n)
-        f1 = rng.uniform(20.0, 100.0)
-        k = int(rng.integers(2, 4))
-        pa1, pa2 = rng.uniform(0.0, 1.5, 2)
-        ups.append(km_unit_parameters(pa1, f1, pa2, k * f1, 0.0, r))
-        coups.append(coupling_from_geometry(pts, r).T.reshape(-1))
-        st = np.zeros((2, n))
-        st[0] = 1.0
-        states.append(st)
-        rtol[:, s] = 1e-8 if s % 2 == 0 else 1e-10
-    return Ensemble(units=units, upar=np.concatenate(ups, axis=1), state=np.concatenate(states, axis=1),
-                    coupling=np.concatenate(coups), matrix_of_system=np.arange(n_systems, dtype=np.int32),
-                    rtol=rtol, atol=rtol.copy(), n_periods=n_periods, reset_at=reset_at,
-                    name=f"c2_{n_systems}_mixed")
+    f1 = rng.uniform(20.0, 100.0, n_systems)
+    k = rng.integers(2, 4, n_systems).astype(np.float64)
+    pa1 = rng.uniform(0.0, 1.5, n_systems)
+    pa2 = rng.uniform(0.0, 1.5, n_systems)
+    off = np.concatenate([[0], np.cumsum(units)[:-1]]).astype(np.int64)
+    tu = int(units.sum())
+    radii = rng.uniform(1.0, 10.0, tu)
+    moff = np.concatenate([[0], np.cumsum(units.astype(np.int64) ** 2)[:-1]])
+    coupling = np.empty(int((units.astype(np.int64) ** 2).sum()))
+    for n in sizes:
+        sys_n = np.nonzero(units == n)[0]
+        if len(sys_n) == 0:
+            continue
+        pts = _ball_points(rng, len(sys_n) * n, sphere_um).reshape(len(sys_n), n, 3)
+        while True:
+            d = np.sqrt(((pts[:, :, None, :] - pts[:, None, :, :]) ** 2).sum(-1))
+            d[:, np.arange(n), np.arange(n)] = np.inf
+            bad = np.triu(d < min_sep_um, 1)
+            if not bad.any():
+                break
+            s_idx, _, j_idx = np.nonzero(bad)
+            pts[s_idx, j_idx] = _ball_points(rng, len(s_idx), sphere_um)
+        r = radii[off[sys_n][:, None] + np.arange(n)[None, :]]            # [m, n]
+        C = (r[:, None, :] ** 3) / (r[:, :, None] ** 2 * d)               # C[s, i, j] = R_j^3 / (R_i^2 d_ij)
+        C[:, np.arange(n), np.arange(n)] = 0.0
+        blocks = np.transpose(C, (0, 2, 1)).reshape(len(sys_n), n * n)     # column-major per system
+        for row, s_ in enumerate(sys_n):
+            coupling[moff[s_]:moff[s_] + n * n] = blocks[row]
+    sys_of_unit = np.repeat(np.arange(n_systems), units)
+    upar = km_unit_parameters(pa1[sys_of_unit], f1[sys_of_unit], pa2[sys_of_unit], (k * f1)[sys_of_unit], 0.0, radii)
+    state = np.zeros((2, tu))
+    state[0] = 1.0
+    tol = np.where(np.arange(n_systems) % 2 == 0, 1e-8, 1e-10)
+    rtol = np.vstack([tol, tol])
+    return Ensemble(units=units, upar=upar, state=state, coupling=coupling,
+                    matrix_of_system=np.arange(n_systems, dtype=np.int32), rtol=rtol, atol=rtol.copy(),
+                    n_periods=n_periods, reset_at=reset_at, name=f"c2_{n_systems}_mixed",
+                    info={"pa1_bar": pa1, "pa2_bar": pa2, "f1_khz": f1, "k": k})
 
 
 def c3_ensemble(n_systems: int = 4096, n_units: int = 128, seed: int = 3, n_periods: int = 4, reset_at: int = -1,

@@ -87,6 +87,8 @@ typedef int32_t bes_status;
 #define BES_OPT_MAX_STEPS_PER_PERIOD 100   /* attempted steps per period before BES_STATUS_STEP_BUDGET (default 1e6) */
 #define BES_OPT_BICG_MAX_ITERATIONS 101    /* the reference's loop runs 19 iterations (Steppers.cuh:508) */
 #define BES_OPT_WARPS_PER_BLOCK 102        /* launch shape: systems (warps) per CTA, 0 = automatic */
+#define BES_OPT_USE_CUDA_GRAPH 103         /* 1 (default): bes_solve_periods captures its launches once into a
+                                              CUDA graph and replays it; 0: direct launches */
 
 /* Algorithms, Interface.cuh:33 */
 #define BES_RK4 0

@@ -9,7 +9,8 @@ O = S.ListOfSolverOptions
 
 
 def run_gpu(ens, n_periods=None, reset_at=None, algorithm=S.Algorithms.RKCK45, ndo=0, do_min_dt=0.0,
-            do_save_frequency=1, per_period_solve=False, warps_per_block=0, bicg_max_iter=19):
+            do_save_frequency=1, per_period_solve=False, warps_per_block=0, bicg_max_iter=19, use_graph=True,
+            repeat=1):
     n_periods = ens.n_periods if n_periods is None else n_periods
     reset_at = ens.reset_at if reset_at is None else reset_at
     ps = ens.make_solver(algorithm=algorithm, n_dense_output=ndo)
@@ -21,6 +22,12 @@ def run_gpu(ens, n_periods=None, reset_at=None, algorithm=S.Algorithms.RKCK45, n
             ps.SolverOption(O.WarpsPerBlock, warps_per_block)
         if bicg_max_iter != 19:
             ps.SolverOption(O.BiCGMaxIterations, bicg_max_iter)
+        if not use_graph:
+            ps.SolverOption(O.UseCudaGraph, 0)
+        for _ in range(repeat - 1):       # earlier solves whose results are discarded (graph capture, replays)
+            ps.SynchroniseFromHostToDevice(V.All)
+            ps.solve_periods(n_periods, reset_at)
+            ps.reset_counters()
         ps.SynchroniseFromHostToDevice(V.All)
         if per_period_solve:
             for p in range(n_periods):

@@ -72,3 +72,10 @@ def test_warps_per_block_does_not_change_results(gpu):
     a = run_gpu(ens, n_periods=1, reset_at=-1, warps_per_block=1)
     b = run_gpu(ens, n_periods=1, reset_at=-1, warps_per_block=4)
     assert_bitwise(a, b, KEYS)
+
+
+def test_graph_replay_equals_direct_launches(gpu):
+    ens = bounded(ragged_ensemble([32, 16, 64, 48, 8, 32, 100], seed=9))
+    direct = run_gpu(ens, n_periods=1, reset_at=-1, use_graph=False)
+    replay = run_gpu(ens, n_periods=1, reset_at=-1, repeat=3)
+    assert_bitwise(replay, direct, KEYS)
