@@ -82,8 +82,8 @@ def parse():
                     help="c1_period1 (default, the headline), c2_period1, c3_period1")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-systems", type=int, default=32)
-    ap.add_argument("--systems", type=int, default=256,
-                    help="profiling only: integrate every (256/S)-th system of the ensemble instead of all 256")
+    ap.add_argument("--systems", type=int, default=0,
+                    help="profiling only: integrate an evenly strided subset of S systems (0: all)")
     return ap.parse_args()
 
 
@@ -208,7 +208,7 @@ def run_b200(args, rank, world, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     ens = make_ensemble(args.workload)
-    if args.systems < ens.n_systems:
+    if 0 < args.systems < ens.n_systems:
         ens = ens.subset(list(range(0, ens.n_systems, ens.n_systems // args.systems))[:args.systems])
     ens.max_steps_per_period = 1_000_000
     ps = ens.make_solver(device=local)
