@@ -92,6 +92,7 @@ struct bes_solver {
     bool order_dirty = true;
     int class_begin[3] = {0, 0, 0}, class_count[3] = {0, 0, 0};
     bool class0_all32 = false;
+    bool class_shared[3] = {false, false, false};   /* every system of the class uses one matrix */
     int sm_count = 148;
     /* the classes run concurrently: fork/join streams, and the whole solve is
      * captured once into a CUDA graph that later calls replay */
@@ -251,6 +252,12 @@ bes_status build_order(bes_solver* h) {
     h->class0_all32 = true;
     for (int i = 0; i < h->class_count[0]; i++)
         if (h->units[idx[i]] != 32) h->class0_all32 = false;
+    for (int c = 0; c < 3; c++) {
+        h->class_shared[c] = h->class_count[c] > 0;
+        for (int i = 1; i < h->class_count[c]; i++)
+            if (h->matrix_of_system[idx[h->class_begin[c] + i]] != h->matrix_of_system[idx[h->class_begin[c]]])
+                h->class_shared[c] = false;
+    }
     if (nact > 0)
         CUDA_TRY(h, cudaMemcpyAsync(h->d_order, h->h_order, sizeof(int32_t) * nact, cudaMemcpyHostToDevice, h->stream));
     h->order_dirty = false;
@@ -313,17 +320,18 @@ struct ClassLaunch {
 /* launch shape of one class (no stream work: safe before a capture) */
 bes_status plan_class(bes_solver* h, int cls, ClassLaunch* L) {
     const int U = cls == 0 ? 1 : (cls == 1 ? 2 : 4);
-    /* N <= 32: operator in registers (2: every system has exactly 32 units) */
-    const int rhs = cls == 0 ? (h->class0_all32 ? 2 : 1) : 0;
+    /* N <= 32: operator in registers (2: every system has exactly 32 units);
+     * larger N: one staged copy of a matrix shared by the whole class when the
+     * caller asked for shared coupling matrices (SharedCouplingMatrices), else W */
+    const int rhs = cls == 0 ? (h->class0_all32 ? 2 : 1) : (h->shared_coupling && h->class_shared[cls] ? 3 : 0);
     const int count = h->class_count[cls];
-    const int smem_warp = (int)bes::warp_smem_bytes(U);
+    const int cap = bes::max_warps_per_block(U, rhs);
     int wpb = h->warps_per_block;
     if (wpb <= 0) {
-        /* spread small ensembles over every SM; fill SMs with 4 warps otherwise */
-        wpb = count <= h->sm_count ? 1 : (count <= 2 * h->sm_count ? 2 : 4);
+        /* spread small ensembles over every SM; fill SMs otherwise */
+        wpb = count <= h->sm_count ? 1 : (count <= 2 * h->sm_count ? 2 : cap);
     }
-    const int max_wpb_smem = (227 * 1024) / smem_warp;
-    wpb = std::max(1, std::min(std::min(wpb, 4), max_wpb_smem));
+    wpb = std::max(1, std::min(wpb, cap));
     int per_sm = 0;
     CUDA_TRY(h, bes::occupancy(U, rhs, wpb, &per_sm));
     if (per_sm < 1)
@@ -630,7 +638,10 @@ bes_status bes_solver_option(bes_solver* h, int32_t option, double value) {
         case BES_OPT_DENSE_OUTPUT_MINIMUM_TIME_STEP: h->do_min_dt = value; break;
         case BES_OPT_DENSE_OUTPUT_SAVE_FREQUENCY: h->do_freq = (int)value; break;
         case BES_OPT_SHARED_GLOBAL_VARIABLES: h->shared_globals = value != 0.0; break;
-        case BES_OPT_SHARED_COUPLING_MATRICES: h->shared_coupling = value != 0.0; break;
+        case BES_OPT_SHARED_COUPLING_MATRICES:
+            h->shared_coupling = value != 0.0;
+            h->order_dirty = true;
+            break;
         case BES_OPT_MAX_STEPS_PER_PERIOD:
             if (!(value >= 1.0)) return fail(h, BES_ERR_ARGUMENT, "SolverOption: MaxStepsPerPeriod must be >= 1");
             h->max_steps = (long long)value;

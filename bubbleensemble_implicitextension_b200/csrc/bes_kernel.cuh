@@ -84,6 +84,22 @@ struct WarpSmem {
                   "broadcast vectors must start on 16-byte boundaries");
 };
 
+/* Shared-memory layout of the shared-matrix variant (RHS = 3): one padded
+ * copy of the launch's coupling matrix per CTA (leading dimension 32U+2:
+ * rows are read lane-consecutive, each lane's column is 16-byte aligned and
+ * its double2 reads are conflict-free), then per warp five broadcast vectors
+ * and the system-scope arrays. */
+template <int U>
+struct SharedCSmem {
+    static constexpr int NMAX = 32 * U;
+    static constexpr int LDC = NMAX + 2;
+    static constexpr int C_DOUBLES = NMAX * LDC;
+    static constexpr int WARP_DOUBLES = (5 * NMAX + NSPa + NSAa + NISAa + 31) / 32 * 32;
+    static constexpr int C_BYTES = C_DOUBLES * 8;
+    static constexpr int WARP_BYTES = WARP_DOUBLES * 8;
+    static_assert(LDC % 2 == 0 && C_DOUBLES % 2 == 0 && WARP_DOUBLES % 2 == 0, "16-byte alignment");
+};
+
 /* halving-tree sum S(L, i) = S(2L, i) + S(2L, i + L), S(P, i) = leaf(i) */
 template <int L, int P>
 struct TreeSum {
@@ -463,6 +479,179 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
     return done;
 }
 
+/* ---------------------------------------------------------------------------
+ * Coupled right-hand side with the launch's shared coupling matrix staged once
+ * per CTA (RHS = 3, U = 2 or 4).  The products apply C to scaled vectors,
+ *   A x0 = rD (C (X1sq x0)),  A p = p + rD (C (X1sq p)),
+ *   A^T p~ = p~ + X1sq (C^T (rD p~)),
+ * with C row sums as four interleaved fma chains and C column sums in the
+ * halving-tree order over 32U; the oracle's shared-matrix association
+ * computes the same. */
+template <int U>
+__device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U>& S, const DeviceProblem& P, double T,
+                                                   double (&Xs)[U][UD], double (&F)[U][UD],
+                                                   double (&up)[U][NUPa], double (&ua)[U][NUAa],
+                                                   int (&iua)[U][NIUAa], bool& capped) {
+    constexpr int NMAX = SharedCSmem<U>::NMAX;
+    constexpr int LDC = SharedCSmem<U>::LDC;
+    constexpr int H = NMAX / 2;
+    const int N = S.N;
+    double xu[U], rd[U], x1[U], r[U], rt[U], x[U], p[U], pt[U];
+    __syncwarp();
+#pragma unroll
+    for (int m = 0; m < U; m++) {
+        const int i = S.lane + 32 * m;
+        if (i < N) {
+            double Fl[UD], cpt, cpf;
+            CoupledSystems_PerBlock_OdeFunction<double>(S.sid, i, Fl, Xs[m], T, up[m], S.sPAR, S.gPAR, S.igPAR,
+                                                        ua[m], iua[m], S.sACC, S.isACC, &cpt, &cpf);
+#pragma unroll
+            for (int k = 0; k < UD; k++) F[m][k] = Fl[k];
+            xu[m] = Fl[IC];
+            rd[m] = cpf;
+            x1[m] = Xs[m][0] * Xs[m][0];
+            S.vcpt[i] = cpt;
+            S.vp[i] = x1[m] * xu[m];   /* z0 = X1sq x0 */
+        } else {
+#pragma unroll
+            for (int k = 0; k < UD; k++) F[m][k] = 0.0;
+            xu[m] = 0.0;
+            rd[m] = 0.0;
+            x1[m] = 0.0;
+            S.vcpt[i] = 0.0;
+            S.vp[i] = 0.0;
+        }
+    }
+    __syncwarp();
+    const double2* cpt2 = reinterpret_cast<const double2*>(S.vcpt);
+    const double2* z2 = reinterpret_cast<const double2*>(S.vp);
+    const double2* zt2 = reinterpret_cast<const double2*>(S.vpt);
+    /* rowsum_m = sum_j C[i_m][j] v[j], four interleaved chains */
+    auto row_sums = [&](const double2* v2, double (&out)[U]) {
+        double a0[U], a1[U], a2[U], a3[U];
+#pragma unroll
+        for (int m = 0; m < U; m++) { a0[m] = 0.0; a1[m] = 0.0; a2[m] = 0.0; a3[m] = 0.0; }
+#pragma unroll 4
+        for (int j = 0; j < NMAX; j += 4) {
+            const double2 va = v2[j / 2], vb = v2[j / 2 + 1];
+#pragma unroll
+            for (int m = 0; m < U; m++) {
+                const double* Crow = S.W + S.lane + 32 * m;
+                if (j < N) a0[m] = fma(Crow[j * LDC], va.x, a0[m]);
+                if (j + 1 < N) a1[m] = fma(Crow[(j + 1) * LDC], va.y, a1[m]);
+                if (j + 2 < N) a2[m] = fma(Crow[(j + 2) * LDC], vb.x, a2[m]);
+                if (j + 3 < N) a3[m] = fma(Crow[(j + 3) * LDC], vb.y, a3[m]);
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < U; m++) out[m] = (a0[m] + a1[m]) + (a2[m] + a3[m]);
+    };
+    double bsum[U], asum[U];
+    row_sums(cpt2, bsum);
+    row_sums(z2, asum);
+#pragma unroll
+    for (int m = 0; m < U; m++) {
+        if (S.lane + 32 * m < N) {
+            const double b = fma(rd[m], bsum[m], xu[m]);
+            const double ax = fma(rd[m], asum[m], xu[m]);
+            r[m] = b - ax;
+        } else {
+            r[m] = 0.0;
+        }
+        rt[m] = r[m];
+        x[m] = xu[m];
+        p[m] = 0.0;
+        pt[m] = 0.0;
+    }
+    double prod[U];
+#pragma unroll
+    for (int m = 0; m < U; m++) prod[m] = r[m] * rt[m];
+    double rho1 = warp_tree_sum<U>(prod);
+    double rho2 = 0.0;
+    int done = 0;
+    bool exited = false;
+    for (int iter = 1; iter <= P.bicg_max_iter; iter++) {
+        if (iter == 1) {
+#pragma unroll
+            for (int m = 0; m < U; m++) { p[m] = r[m]; pt[m] = rt[m]; }
+            if (fabs(rho1) < 1e-6) { exited = true; break; }
+        } else {
+            const double beta = rho1 / rho2;
+#pragma unroll
+            for (int m = 0; m < U; m++) {
+                p[m] = fma(beta, p[m], r[m]);
+                pt[m] = fma(beta, pt[m], rt[m]);
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int m = 0; m < U; m++) {
+            const int i = S.lane + 32 * m;
+            S.vp[i] = x1[m] * p[m];    /* z  = X1sq p  */
+            S.vpt[i] = rd[m] * pt[m];  /* z~ = rD p~   */
+        }
+        __syncwarp();
+        double qs[U], qts[U];
+        row_sums(z2, qs);
+#pragma unroll
+        for (int m = 0; m < U; m++) {
+            /* column i_m of C against z~: the first tree levels on the loads, then the halving tree over 32 */
+            const double2* Ccol2 = reinterpret_cast<const double2*>(S.W + (S.lane + 32 * m) * LDC);
+            double u[32];
+#pragma unroll
+            for (int k = 0; k < 32; k += 2) {
+                double2 c0 = Ccol2[k / 2], z0 = zt2[k / 2];
+                double s0 = c0.x * z0.x, s1 = c0.y * z0.y;
+                if constexpr (H >= 32) {
+                    const double2 c1 = Ccol2[(k + 32) / 2], z1 = zt2[(k + 32) / 2];
+                    if constexpr (H == 64) {
+                        const double2 c2 = Ccol2[(k + 64) / 2], zz2 = zt2[(k + 64) / 2];
+                        const double2 c3 = Ccol2[(k + 96) / 2], z3 = zt2[(k + 96) / 2];
+                        s0 = (s0 + c2.x * zz2.x) + (c1.x * z1.x + c3.x * z3.x);
+                        s1 = (s1 + c2.y * zz2.y) + (c1.y * z1.y + c3.y * z3.y);
+                    } else {
+                        s0 = s0 + c1.x * z1.x;
+                        s1 = s1 + c1.y * z1.y;
+                    }
+                }
+                u[k] = s0;
+                u[k + 1] = s1;
+            }
+            auto leaf = [&](int k) -> double { return u[k]; };
+            qts[m] = TreeSum<1, 32>::run(0, leaf);
+        }
+        double q[U], qt[U];
+#pragma unroll
+        for (int m = 0; m < U; m++) {
+            const bool v = S.lane + 32 * m < N;
+            q[m] = v ? fma(rd[m], qs[m], p[m]) : 0.0;
+            qt[m] = v ? fma(x1[m], qts[m], pt[m]) : 0.0;
+        }
+#pragma unroll
+        for (int m = 0; m < U; m++) prod[m] = pt[m] * q[m];
+        const double alpha = rho1 / warp_tree_sum<U>(prod);
+        double ar[U];
+#pragma unroll
+        for (int m = 0; m < U; m++) {
+            x[m] = fma(alpha, p[m], x[m]);
+            r[m] = fma(-alpha, q[m], r[m]);
+            rt[m] = fma(-alpha, qt[m], rt[m]);
+            ar[m] = fabs(r[m]);
+            prod[m] = r[m] * rt[m];
+        }
+        double rmax, rho_next;
+        warp_tree_max_sum<U>(ar, prod, rmax, rho_next);
+        rho2 = rho1;
+        done++;
+        if (rmax < 1e-6) { exited = true; break; }
+        rho1 = rho_next;
+    }
+    if (!exited) capped = true;
+#pragma unroll
+    for (int m = 0; m < U; m++) F[m][IC] = x[m];
+    return done;
+}
+
 /* the right-hand side a kernel variant uses */
 template <int U, int RHS>
 __device__ __forceinline__ int rhs_eval(const Sys<U>& S, const DeviceProblem& P, double T, double (&Xs)[U][UD],
@@ -470,6 +659,8 @@ __device__ __forceinline__ int rhs_eval(const Sys<U>& S, const DeviceProblem& P,
                                         int (&iua)[U][NIUAa], bool& capped) {
     if constexpr (RHS == 0) {
         return coupled_rhs<U>(S, P, T, Xs, F, up, ua, iua, capped);
+    } else if constexpr (RHS == 3) {
+        return coupled_rhs_sharedc<U>(S, P, T, Xs, F, up, ua, iua, capped);
     } else {
         static_assert(U == 1, "the register-resident operator needs one unit per lane");
         return coupled_rhs_regw<RHS == 2 ? 32 : 0>(S, P, T, Xs, F, up, ua, iua, capped);
@@ -497,7 +688,7 @@ __device__ __forceinline__ bool valid_unit(const Sys<U>& S, int m) { return S.la
 /* the parameter array a callback gets for slot m of this lane */
 template <int U, int RHS>
 __device__ __forceinline__ double* upar_of(const Sys<U>& S, Lane<U>& L, int m) {
-    if constexpr (RHS != 0) return S.upsh + (S.lane + 32 * m) * NUPa;
+    if constexpr (RHS == 1 || RHS == 2) return S.upsh + (S.lane + 32 * m) * NUPa;
     else return L.up[m];
 }
 
@@ -928,27 +1119,53 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
 /* ---------------------------------------------------------------------------
  * The kernel: warps pull systems from the work counter.
  * RHS = 0: operator W in shared memory (any U); RHS = 1 / 2: operator in
- * registers (U = 1; 2 = every system of the launch has exactly 32 units). */
+ * registers (U = 1; 2 = every system of the launch has exactly 32 units);
+ * RHS = 3: every system of the launch shares one coupling matrix, staged once
+ * per CTA (U = 2, 4; up to 8 warps per CTA). */
 template <int U, int RHS>
-__global__ void __launch_bounds__(128) bes_ensemble_kernel(DeviceProblem P) {
+__global__ void __launch_bounds__(RHS == 3 ? 256 : 128, 1) bes_ensemble_kernel(DeviceProblem P) {
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    double* base = smem + (size_t)wib * WarpSmem<U>::DOUBLES;
     Sys<U> S;
     S.lane = lane;
     S.tot = P.total_units;
-    S.W = base;
-    S.vp = base + WarpSmem<U>::W_DOUBLES;
-    S.vpt = S.vp + WarpSmem<U>::NMAX;
-    S.vcpt = S.vpt + WarpSmem<U>::NMAX;
-    S.vx1 = S.vcpt + WarpSmem<U>::NMAX;
-    S.vxu = S.vx1 + WarpSmem<U>::NMAX;
-    S.vrd = S.vxu + WarpSmem<U>::NMAX;
-    S.sPAR = S.vrd + WarpSmem<U>::NMAX;
+    if constexpr (RHS == 3) {
+        /* one copy of the launch's shared coupling matrix per CTA, zero-padded */
+        constexpr int LDC = SharedCSmem<U>::LDC;
+        const int s0 = P.order[0];
+        const int n0 = P.units[s0];
+        const double* Cg = P.coupling + P.coupling_offset[s0];
+        for (int idx = threadIdx.x; idx < SharedCSmem<U>::C_DOUBLES; idx += blockDim.x) {
+            const int r = idx % LDC, c = idx / LDC;
+            smem[idx] = (r < n0 && c < n0) ? __ldg(Cg + r + (int64_t)c * n0) : 0.0;
+        }
+        __syncthreads();
+        constexpr int NM = SharedCSmem<U>::NMAX;
+        double* base = smem + SharedCSmem<U>::C_DOUBLES + (size_t)wib * SharedCSmem<U>::WARP_DOUBLES;
+        S.W = smem;
+        S.vp = base;
+        S.vpt = base + NM;
+        S.vcpt = base + 2 * NM;
+        S.vx1 = base + 3 * NM;
+        S.vxu = base + 4 * NM;
+        S.vrd = nullptr;
+        S.sPAR = base + 5 * NM;
+        S.upsh = nullptr;
+    } else {
+        double* base = smem + (size_t)wib * WarpSmem<U>::DOUBLES;
+        S.W = base;
+        S.vp = base + WarpSmem<U>::W_DOUBLES;
+        S.vpt = S.vp + WarpSmem<U>::NMAX;
+        S.vcpt = S.vpt + WarpSmem<U>::NMAX;
+        S.vx1 = S.vcpt + WarpSmem<U>::NMAX;
+        S.vxu = S.vx1 + WarpSmem<U>::NMAX;
+        S.vrd = S.vxu + WarpSmem<U>::NMAX;
+        S.sPAR = S.vrd + WarpSmem<U>::NMAX;
+        S.upsh = S.sPAR + WarpSmem<U>::SYS_DOUBLES;
+    }
     S.sACC = S.sPAR + NSPa;
     S.isACC = reinterpret_cast<int*>(S.sACC + NSAa);
-    S.upsh = S.sPAR + WarpSmem<U>::SYS_DOUBLES;
     S.gPAR = P.gpar;
     S.igPAR = P.igpar;
 
@@ -971,7 +1188,7 @@ __global__ void __launch_bounds__(128) bes_ensemble_kernel(DeviceProblem P) {
             const int64_t g = S.off + i;
 #pragma unroll
             for (int c = 0; c < UD; c++) L.X[m][c] = v ? P.state[(int64_t)c * S.tot + g] : 0.0;
-            if constexpr (RHS != 0) {
+            if constexpr (RHS == 1 || RHS == 2) {
                 for (int c = 0; c < NUP; c++) S.upsh[i * NUPa + c] = v ? __ldg(P.upar + (int64_t)c * S.tot + g) : 0.0;
             } else {
 #pragma unroll
@@ -985,7 +1202,7 @@ __global__ void __launch_bounds__(128) bes_ensemble_kernel(DeviceProblem P) {
         for (int c = lane; c < NSP; c += 32) S.sPAR[c] = P.spar[(int64_t)c * P.n_systems + sid];
         for (int c = lane; c < NSA; c += 32) S.sACC[c] = P.sacc[(int64_t)c * P.n_systems + sid];
         for (int c = lane; c < NISA; c += 32) S.isACC[c] = P.isacc[(int64_t)c * P.n_systems + sid];
-        if constexpr (RHS != 0) {
+        if constexpr (RHS == 1 || RHS == 2) {
             /* stage the system's coupling matrix, zero-padded to 32 x 33 */
             constexpr int LDC = WarpSmem<1>::LDW;
             for (int idx = lane; idx < 32 * LDC; idx += 32) {

@@ -5,10 +5,12 @@
 
 namespace bes {
 
+template <>
+size_t cta_smem_t<1, 1>(int warps) { return (size_t)warps * WarpSmem<1>::BYTES; }
 
 template <>
 cudaError_t occupancy_t<1, 1>(int warps, int* ctas_per_sm) {
-    const size_t smem = (size_t)warps * WarpSmem<1>::BYTES;
+    const size_t smem = cta_smem_t<1, 1>(warps);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(bes_ensemble_kernel<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
@@ -19,14 +21,15 @@ cudaError_t occupancy_t<1, 1>(int warps, int* ctas_per_sm) {
 
 template <>
 cudaError_t launch_t<1, 1>(const DeviceProblem& P, int grid, int warps, cudaStream_t stream) {
-    const size_t smem = (size_t)warps * WarpSmem<1>::BYTES;
-    bes_ensemble_kernel<1, 1><<<grid, 32 * warps, smem, stream>>>(P);
+    bes_ensemble_kernel<1, 1><<<grid, 32 * warps, cta_smem_t<1, 1>(warps), stream>>>(P);
     return cudaGetLastError();
 }
+template <>
+size_t cta_smem_t<1, 2>(int warps) { return (size_t)warps * WarpSmem<1>::BYTES; }
 
 template <>
 cudaError_t occupancy_t<1, 2>(int warps, int* ctas_per_sm) {
-    const size_t smem = (size_t)warps * WarpSmem<1>::BYTES;
+    const size_t smem = cta_smem_t<1, 2>(warps);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(bes_ensemble_kernel<1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
@@ -37,9 +40,7 @@ cudaError_t occupancy_t<1, 2>(int warps, int* ctas_per_sm) {
 
 template <>
 cudaError_t launch_t<1, 2>(const DeviceProblem& P, int grid, int warps, cudaStream_t stream) {
-    const size_t smem = (size_t)warps * WarpSmem<1>::BYTES;
-    bes_ensemble_kernel<1, 2><<<grid, 32 * warps, smem, stream>>>(P);
+    bes_ensemble_kernel<1, 2><<<grid, 32 * warps, cta_smem_t<1, 2>(warps), stream>>>(P);
     return cudaGetLastError();
 }
-
 }  // namespace bes

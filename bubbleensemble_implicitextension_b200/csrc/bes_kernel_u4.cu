@@ -5,10 +5,12 @@
 
 namespace bes {
 
+template <>
+size_t cta_smem_t<4, 0>(int warps) { return (size_t)warps * WarpSmem<4>::BYTES; }
 
 template <>
 cudaError_t occupancy_t<4, 0>(int warps, int* ctas_per_sm) {
-    const size_t smem = (size_t)warps * WarpSmem<4>::BYTES;
+    const size_t smem = cta_smem_t<4, 0>(warps);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(bes_ensemble_kernel<4, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
@@ -19,9 +21,26 @@ cudaError_t occupancy_t<4, 0>(int warps, int* ctas_per_sm) {
 
 template <>
 cudaError_t launch_t<4, 0>(const DeviceProblem& P, int grid, int warps, cudaStream_t stream) {
-    const size_t smem = (size_t)warps * WarpSmem<4>::BYTES;
-    bes_ensemble_kernel<4, 0><<<grid, 32 * warps, smem, stream>>>(P);
+    bes_ensemble_kernel<4, 0><<<grid, 32 * warps, cta_smem_t<4, 0>(warps), stream>>>(P);
     return cudaGetLastError();
 }
+template <>
+size_t cta_smem_t<4, 3>(int warps) { return (size_t)SharedCSmem<4>::C_BYTES + (size_t)warps * SharedCSmem<4>::WARP_BYTES; }
 
+template <>
+cudaError_t occupancy_t<4, 3>(int warps, int* ctas_per_sm) {
+    const size_t smem = cta_smem_t<4, 3>(warps);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(bes_ensemble_kernel<4, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, bes_ensemble_kernel<4, 3>, 32 * warps, smem);
+}
+
+template <>
+cudaError_t launch_t<4, 3>(const DeviceProblem& P, int grid, int warps, cudaStream_t stream) {
+    bes_ensemble_kernel<4, 3><<<grid, 32 * warps, cta_smem_t<4, 3>(warps), stream>>>(P);
+    return cudaGetLastError();
+}
 }  // namespace bes

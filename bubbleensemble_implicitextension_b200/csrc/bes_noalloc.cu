@@ -183,11 +183,10 @@ extern "C" bes_status bes_solve_periods_noalloc(const bes_noalloc_problem* p, in
         P.order = scratch + 4 + begin[cls];
         P.n_active = count[cls];
         P.work_counter = scratch + cls;
+        const int cap = bes::max_warps_per_block(U, rhs);
         int wpb = p->warps_per_block > 0 ? p->warps_per_block
-                                          : (count[cls] <= sms ? 1 : (count[cls] <= 2 * sms ? 2 : 4));
-        const int max_wpb = (int)((227 * 1024) / bes::warp_smem_bytes(U));
-        wpb = wpb < 1 ? 1 : (wpb > 4 ? 4 : wpb);
-        if (wpb > max_wpb) wpb = max_wpb < 1 ? 1 : max_wpb;
+                                          : (count[cls] <= sms ? 1 : (count[cls] <= 2 * sms ? 2 : cap));
+        wpb = wpb < 1 ? 1 : (wpb > cap ? cap : wpb);
         int per_sm = 0;
         e = bes::occupancy(U, rhs, wpb, &per_sm);
         if (e != cudaSuccess || per_sm < 1)

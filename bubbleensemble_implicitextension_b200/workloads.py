@@ -138,6 +138,7 @@ class Ensemble:
     n_periods: int = 64
     reset_at: int = 32
     max_steps_per_period: int = 1_000_000
+    shared_matrices: bool = False     # SharedCouplingMatrices: stage the launch's one matrix per CTA
     name: str = ""
     info: dict = dataclasses.field(default_factory=dict)
 
@@ -222,6 +223,8 @@ class Ensemble:
         ps.SolverOption(O.EventDirection, 0, self.event_dir)
         ps.SolverOption(O.MaxStepsPerPeriod, self.max_steps_per_period)
         ps.set_accessory_reset(np.zeros(NUA), np.array([-1], dtype=np.int32))
+        if self.shared_matrices:
+            ps.SolverOption(O.SharedCouplingMatrices, 1)
 
 
 def c1_ensemble(n_pa: int = 16, n_f: int = 16, n_units: int = 32, spacing_um: float = 150.0,
@@ -327,7 +330,7 @@ def c3_ensemble(n_systems: int = 4096, n_units: int = 128, seed: int = 3, n_peri
     return Ensemble(units=np.full(n_systems, n_units, dtype=np.int32), upar=upar, state=state,
                     coupling=C.T.reshape(-1).copy(), matrix_of_system=np.zeros(n_systems, dtype=np.int32),
                     rtol=np.full((2, n_systems), rtol), atol=np.full((2, n_systems), rtol), n_periods=n_periods,
-                    reset_at=reset_at, name=f"c3_{n_systems}x{n_units}_shared")
+                    reset_at=reset_at, shared_matrices=True, name=f"c3_{n_systems}x{n_units}_shared")
 
 
 def collapse_records(uacc: np.ndarray, iuacc: np.ndarray, units: np.ndarray):

@@ -18,6 +18,12 @@
  *     combined as (s0 + s1) + (s2 + s3) (a shorter dependency chain on the
  *     GPU); A*p adds that sum to p_i;
  *   - the operator element is W_ij = (rD_i * C_ij) * X1sq_j (Steppers.cuh:685).
+ *   - shared-matrix association (systems with N > 32 whose coupling matrix is
+ *     shared by the launch and staged once in shared memory): the products
+ *     apply C to a scaled vector instead of forming W,
+ *       A x0:  rD_i * sum_j C_ij (X1sq_j x0_j)        (fma chains as above)
+ *       A p:   p_i + rD_i * sum_j C_ij (X1sq_j p_j)
+ *       A^T p~: p~_i + X1sq_i * tree_j C_ji (rD_j p~_j).
  * The product kernel follows the same order, so oracle and kernel agree
  * bit for bit.
  */
@@ -128,7 +134,7 @@ struct Work {
  * iteration limit was used up without meeting an exit test. */
 int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
                 const double* up, long ups, const double* C, int max_iter,
-                double* f0, double* f1, bool* capped) {
+                double* f0, double* f1, bool* capped, bool shared_assoc = false) {
     const int N = w.N;
     double upl[NUP];
     for (int i = 0; i < N; i++) {
@@ -140,7 +146,9 @@ int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
     for (int i = 0; i < N; i++) {
         double bi = row_sum4(N, [&](int j) { return C[i + (long)j * N]; }, [&](int j) { return w.cpt[j]; });
         bi = fma(w.rd[i], bi, w.xu[i]);
-        double ax = row_sum4(N, [&](int j) { return C[i + (long)j * N] * w.x1sq[j]; }, [&](int j) { return w.xu[j]; });
+        double ax = shared_assoc
+                        ? row_sum4(N, [&](int j) { return C[i + (long)j * N]; }, [&](int j) { return w.x1sq[j] * w.xu[j]; })
+                        : row_sum4(N, [&](int j) { return C[i + (long)j * N] * w.x1sq[j]; }, [&](int j) { return w.xu[j]; });
         ax = fma(w.rd[i], ax, w.xu[i]);
         w.r[i] = bi - ax;
         w.rt[i] = w.r[i];
@@ -164,10 +172,21 @@ int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
             }
         }
         /* q = A p (row sums) and qt = A^T pt (tree sums), Steppers.cuh:669-706 */
+        if (shared_assoc) {
+            for (int j = 0; j < N; j++) { w.b[j] = w.x1sq[j] * w.p[j]; w.xu[j] = w.rd[j] * w.pt[j]; }
+            /* w.b, w.xu reused as the scaled vectors z = X1sq p and z~ = rD p~ (x_u is no longer needed) */
+        }
         for (int i = 0; i < N; i++) {
-            w.q[i] = w.p[i] + row_sum4(N, [&](int j) { return w.W[i + (long)j * N]; }, [&](int j) { return w.p[j]; });
-            for (int j = 0; j < N; j++) w.tmp2[j] = w.W[j + (long)i * N] * w.pt[j];
-            w.qt[i] = w.pt[i] + tree_sum(w.tmp2.data(), N, w.tmp.data());
+            if (shared_assoc) {
+                double s = row_sum4(N, [&](int j) { return C[i + (long)j * N]; }, [&](int j) { return w.b[j]; });
+                w.q[i] = fma(w.rd[i], s, w.p[i]);
+                for (int j = 0; j < N; j++) w.tmp2[j] = C[j + (long)i * N] * w.xu[j];
+                w.qt[i] = fma(w.x1sq[i], tree_sum(w.tmp2.data(), N, w.tmp.data()), w.pt[i]);
+            } else {
+                w.q[i] = w.p[i] + row_sum4(N, [&](int j) { return w.W[i + (long)j * N]; }, [&](int j) { return w.p[j]; });
+                for (int j = 0; j < N; j++) w.tmp2[j] = w.W[j + (long)i * N] * w.pt[j];
+                w.qt[i] = w.pt[i] + tree_sum(w.tmp2.data(), N, w.tmp.data());
+            }
         }
         for (int i = 0; i < N; i++) w.tmp2[i] = w.pt[i] * w.q[i];
         double alpha = rho1 / tree_sum(w.tmp2.data(), N, w.tmp.data());
@@ -224,7 +243,8 @@ struct SystemRun {
 
     int rhs(double T, const double* a0, const double* a1, double* f0, double* f1, int64_t& nbicg, bool& capped_any) {
         bool capped = false;
-        int it = coupled_rhs(w, T, a0, a1, up(), tot, C(), P->bicg_max_iter, f0, f1, &capped);
+        int it = coupled_rhs(w, T, a0, a1, up(), tot, C(), P->bicg_max_iter, f0, f1, &capped,
+                             P->shared_assoc != 0 && N > 32);
         nbicg += it;
         if (capped) capped_any = true;
         return it;

@@ -65,7 +65,7 @@ typedef struct bes_oracle_problem {
     int32_t algorithm;               /* 0 = RK4, 1 = RKCK45 */
     double dt0, dtmin, dtmax, grow, shrink;
     int32_t bicg_max_iter;           /* the reference's loop runs iter = 1..19 */
-    int32_t pad0;
+    int32_t shared_assoc;            /* 1: systems with N > 32 use the shared-matrix association (see .cpp) */
     int64_t max_steps_per_period;    /* attempted steps per period before STEP_BUDGET */
     int32_t ndo;                     /* dense output slots per system */
     int32_t do_save_frequency;

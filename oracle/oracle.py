@@ -31,7 +31,7 @@ class Problem(ctypes.Structure):
         ("event_tol", ctypes.c_double), ("event_dir", ctypes.c_int32), ("algorithm", ctypes.c_int32),
         ("dt0", ctypes.c_double), ("dtmin", ctypes.c_double), ("dtmax", ctypes.c_double),
         ("grow", ctypes.c_double), ("shrink", ctypes.c_double),
-        ("bicg_max_iter", ctypes.c_int32), ("pad0", ctypes.c_int32), ("max_steps_per_period", ctypes.c_int64),
+        ("bicg_max_iter", ctypes.c_int32), ("shared_assoc", ctypes.c_int32), ("max_steps_per_period", ctypes.c_int64),
         ("ndo", ctypes.c_int32), ("do_save_frequency", ctypes.c_int32), ("do_min_dt", ctypes.c_double),
         ("dense_time", _dp), ("dense_state", _dp), ("dense_index", _i32p),
         ("n_accepted", _i64p), ("n_rejected", _i64p), ("n_bicg_iter", _i64p), ("n_rhs", _i64p),
@@ -79,7 +79,7 @@ def _p(a, t):
 
 def run(ens, n_periods: int = None, reset_at: int = None, threads: int = 0, systems=None,
         algorithm: int = 1, ndo: int = 0, do_min_dt: float = 0.0, do_save_frequency: int = 1,
-        bicg_max_iter: int = 19, uacc=None, iuacc=None, state=None) -> dict:
+        bicg_max_iter: int = 19, uacc=None, iuacc=None, state=None, shared_assoc=None) -> dict:
     """Integrate an ``workloads.Ensemble`` on the CPU; returns the final arrays and counters."""
     if systems is not None:
         ens = ens.subset(systems)
@@ -127,6 +127,9 @@ def run(ens, n_periods: int = None, reset_at: int = None, threads: int = 0, syst
     P.algorithm = algorithm
     P.dt0, P.dtmin, P.dtmax, P.grow, P.shrink = ens.dt0, ens.dtmin, ens.dtmax, ens.grow, ens.shrink
     P.bicg_max_iter = bicg_max_iter
+    # the library stages a launch's one shared matrix per CTA (and associates the products
+    # accordingly) when the ensemble asks for shared coupling matrices
+    P.shared_assoc = int(getattr(ens, "shared_matrices", False) if shared_assoc is None else shared_assoc)
     P.max_steps_per_period = ens.max_steps_per_period
     P.ndo = ndo
     P.do_save_frequency = do_save_frequency

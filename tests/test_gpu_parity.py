@@ -79,3 +79,14 @@ def test_graph_replay_equals_direct_launches(gpu):
     direct = run_gpu(ens, n_periods=1, reset_at=-1, use_graph=False)
     replay = run_gpu(ens, n_periods=1, reset_at=-1, repeat=3)
     assert_bitwise(replay, direct, KEYS)
+
+
+@pytest.mark.parametrize("n,seed", [(128, 31), (100, 32), (64, 33), (48, 34)])
+def test_shared_matrix_staged_per_cta(n, seed, gpu, oracle_lib):
+    """SharedCouplingMatrices on: one matrix for the whole launch, staged once per
+    CTA; the products follow the oracle's shared-matrix association."""
+    ens = bounded(W.c3_ensemble(n_systems=6, n_units=n, seed=seed, pa_bar=1.0, f_khz=150.0, n_periods=1,
+                                reset_at=-1, cube_um=400.0 * (n / 32) ** (1 / 3)))
+    got = run_gpu(ens, n_periods=1, reset_at=-1, shared_matrices=True, warps_per_block=4)
+    want = oracle_lib.run(ens, n_periods=1, reset_at=-1, shared_assoc=True)
+    assert_bitwise(got, want, KEYS)
