@@ -18,7 +18,7 @@ INCLUDE = PKG.parent / "include"
 BUILD = PKG / "_build"
 LIB = PKG / "libbes.so"
 
-SOURCES = ["bes_api.cu", "bes_launch.cu", "bes_peak.cu", "bes_noalloc.cu", "bes_kernel_u1.cu", "bes_kernel_u2.cu", "bes_kernel_u4.cu"]
+SOURCES = ["bes_api.cu", "bes_launch.cu", "bes_peak.cu", "bes_noalloc.cu", "bes_mlp.cu", "bes_kernel_u1.cu", "bes_kernel_u2.cu", "bes_kernel_u4.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",

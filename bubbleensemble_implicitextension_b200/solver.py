@@ -138,6 +138,12 @@ class CountersStruct(ctypes.Structure):
     ]
 
 
+class MlpConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("n_in", ctypes.c_int32), ("width", ctypes.c_int32),
+                ("depth", ctypes.c_int32), ("n_out", ctypes.c_int32), ("max_batch", ctypes.c_int32),
+                ("seed", ctypes.c_uint64)]
+
+
 class NoallocProblem(ctypes.Structure):
     """bes_noalloc_problem (include/bes.h): device pointers of a caller-owned ensemble."""
     _P64 = ctypes.c_void_p
@@ -203,6 +209,18 @@ SIGNATURES = {
     "bes_device_info_get": [_I32, ctypes.POINTER(DeviceInfo)],
     "bes_measure_fp64_peak": [_I32, ctypes.POINTER(ctypes.c_double)],
     "bes_solve_periods_noalloc": [ctypes.POINTER(NoallocProblem), _I32, _I32, _P],
+    "bes_mlp_create": [ctypes.POINTER(MlpConfig), ctypes.POINTER(ctypes.c_void_p)],
+    "bes_mlp_destroy": [_P],
+    "bes_mlp_parameter_count": [_P, ctypes.POINTER(ctypes.c_int64)],
+    "bes_mlp_set_normalization": [_P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                                  ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)],
+    "bes_mlp_get_parameters": [_P, ctypes.POINTER(ctypes.c_float), ctypes.c_int64],
+    "bes_mlp_set_parameters": [_P, ctypes.POINTER(ctypes.c_float), ctypes.c_int64],
+    "bes_mlp_get_gradients": [_P, ctypes.POINTER(ctypes.c_float), ctypes.c_int64],
+    "bes_mlp_forward": [_P, _P, _I32, _P, _P],
+    "bes_mlp_backward": [_P, _P, _P, _I32, ctypes.POINTER(ctypes.c_float), _P],
+    "bes_mlp_adam_step": [_P, ctypes.c_float, _P],
+    "bes_mlp_last_error": [_P],
     "bes_status_string": [_I32],
     "bes_last_error": [_P],
 }
@@ -222,7 +240,8 @@ def load_library(path: Optional[os.PathLike] = None) -> ctypes.CDLL:
     for name, args in SIGNATURES.items():
         fn = getattr(lib, name)
         fn.argtypes = args
-        fn.restype = ctypes.c_char_p if name in ("bes_status_string", "bes_last_error") else ctypes.c_int32
+        fn.restype = (ctypes.c_char_p if name in ("bes_status_string", "bes_last_error", "bes_mlp_last_error")
+                      else ctypes.c_int32)
     if path is None:
         _lib = lib
     return lib

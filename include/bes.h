@@ -321,6 +321,36 @@ typedef struct bes_noalloc_problem {
 bes_status bes_solve_periods_noalloc(const bes_noalloc_problem* problem, int32_t n_periods, int32_t reset_at,
                                      void* stream);
 
+/* ---- surrogate network (no reference counterpart) -------------------------
+ * A small MLP (n_in -> width x depth (GELU) -> n_out) trained and evaluated
+ * by the library's own CUDA kernels: BF16 weights and activations, FP32
+ * master weights, FP32 accumulation, Adam.  It maps sweep parameters
+ * (amplitude, frequency, radius statistics) to collapse outputs so that a
+ * sweep integrates only the points it flags.  x, y, target are device
+ * pointers to row-major [batch][n] FP32 arrays. */
+typedef struct bes_mlp bes_mlp;
+typedef struct bes_mlp_config {
+    int32_t device;
+    int32_t n_in, width, depth, n_out;
+    int32_t max_batch;
+    uint64_t seed;
+} bes_mlp_config;
+bes_status bes_mlp_create(const bes_mlp_config* config, bes_mlp** out);
+bes_status bes_mlp_destroy(bes_mlp* m);
+bes_status bes_mlp_parameter_count(bes_mlp* m, int64_t* count);
+/* standardisation of inputs and targets (host arrays) */
+bes_status bes_mlp_set_normalization(bes_mlp* m, const float* in_mean, const float* in_std, const float* out_mean,
+                                     const float* out_std);
+bes_status bes_mlp_get_parameters(bes_mlp* m, float* host, int64_t count);
+bes_status bes_mlp_set_parameters(bes_mlp* m, const float* host, int64_t count);
+bes_status bes_mlp_get_gradients(bes_mlp* m, float* host, int64_t count);
+bes_status bes_mlp_forward(bes_mlp* m, const float* x, int32_t batch, float* y, void* stream);
+/* gradients of the mean squared error of the standardised outputs; loss (host) optional */
+bes_status bes_mlp_backward(bes_mlp* m, const float* x, const float* target, int32_t batch, float* loss,
+                            void* stream);
+bes_status bes_mlp_adam_step(bes_mlp* m, float learning_rate, void* stream);
+const char* bes_mlp_last_error(const bes_mlp* m);
+
 const char* bes_status_string(bes_status status);
 const char* bes_last_error(const bes_solver* h);
 
