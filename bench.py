@@ -210,7 +210,9 @@ def run_b200(args, rank, world, local):
     ens = make_ensemble(args.workload)
     if 0 < args.systems < ens.n_systems:
         ens = ens.subset(list(range(0, ens.n_systems, ens.n_systems // args.systems))[:args.systems])
-    ens.max_steps_per_period = 1_000_000
+    # step budget per period: 4.4x the slowest system of c1_period1 and ~4x the 99th percentile of
+    # c2_period1; a system that needs more (the minimum-step cases) is cut short and counted
+    ens.max_steps_per_period = 50_000
     ps = ens.make_solver(device=local)
     stream = torch.cuda.current_stream(dev)
     ps.set_stream(stream.cuda_stream)
@@ -317,7 +319,9 @@ def run_b200(args, rank, world, local):
         "gpu_launches": launches,
         "clocks": clk,
         "counters": {"attempted_steps": int(attempted.sum()), "max_attempted_steps": int(attempted.max()),
-                     "bicg_iterations": int(c["bicg"].sum()), "status_or": int(np.bitwise_or.reduce(c["status"]))},
+                     "bicg_iterations": int(c["bicg"].sum()), "status_or": int(np.bitwise_or.reduce(c["status"])),
+                     "systems_at_step_budget": int(((c["status"] & 4) > 0).sum()),
+                     "step_budget_per_period": int(ens.max_steps_per_period)},
     }
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(ens, args.cpu_sample_systems)

@@ -244,7 +244,7 @@ def screen_sweep(mlp: MLP, pa: np.ndarray, f_khz: np.ndarray, radii_um: np.ndarr
     t0 = time.perf_counter()
     PA, FR = np.meshgrid(pa, f_khz, indexing="ij")
     X = features(PA.ravel(), FR.ravel(), radii_um)
-    pred = mlp.predict(X).reshape(len(pa), len(f_khz), 2)
+    pred = mlp.predict(X).reshape(len(pa), len(f_khz), 2).astype(np.float64)
     m = pred[..., 0]
     jump = np.zeros_like(m)
     jump[1:, :] = np.maximum(jump[1:, :], np.abs(m[1:, :] - m[:-1, :]))
