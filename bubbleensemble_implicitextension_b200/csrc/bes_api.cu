@@ -102,6 +102,7 @@ struct bes_solver {
     int g_periods = -1, g_reset = -2, g_launches = 0;
     bool graph_dirty = true;
     int use_graph = 1;
+    int warps_per_system = 0;   /* 0: multi-warp systems above 32 units; 1: one warp per system */
     float last_ms = 0.f;
     int last_launches = 0;
     std::string err;
@@ -314,31 +315,26 @@ DeviceProblem make_problem(bes_solver* h) {
 }
 
 struct ClassLaunch {
-    int U, rhs, grid, wpb;
+    bes::Variant v;
+    int grid, wpb;
 };
 
 /* launch shape of one class (no stream work: safe before a capture) */
 bes_status plan_class(bes_solver* h, int cls, ClassLaunch* L) {
-    const int U = cls == 0 ? 1 : (cls == 1 ? 2 : 4);
-    /* N <= 32: operator in registers (2: every system has exactly 32 units);
-     * larger N: one staged copy of a matrix shared by the whole class when the
-     * caller asked for shared coupling matrices (SharedCouplingMatrices), else W */
-    const int rhs = cls == 0 ? (h->class0_all32 ? 2 : 1) : (h->shared_coupling && h->class_shared[cls] ? 3 : 0);
+    const bes::Variant v = bes::class_variant(cls, h->class0_all32, h->shared_coupling && h->class_shared[cls],
+                                         h->warps_per_system);
     const int count = h->class_count[cls];
-    const int cap = bes::max_warps_per_block(U, rhs);
-    int wpb = h->warps_per_block;
-    if (wpb <= 0) {
-        /* spread small ensembles over every SM; fill SMs otherwise */
-        wpb = count <= h->sm_count ? 1 : (count <= 2 * h->sm_count ? 2 : cap);
-    }
-    wpb = std::max(1, std::min(wpb, cap));
+    if (bes::max_warps_per_block(v) < v.G)
+        return fail(h, BES_ERR_CUDA, "solver kernel variant (U=%d, G=%d) does not fit in shared memory", v.U, v.G);
+    const int wpb = bes::class_warps_per_block(v, count, h->sm_count, h->warps_per_block);
     int per_sm = 0;
-    CUDA_TRY(h, bes::occupancy(U, rhs, wpb, &per_sm));
+    CUDA_TRY(h, bes::occupancy(v, wpb, &per_sm));
     if (per_sm < 1)
-        return fail(h, BES_ERR_CUDA, "solver kernel (U=%d) cannot be resident with %d warps per block", U, wpb);
-    const int needed = (count + wpb - 1) / wpb;
-    L->U = U;
-    L->rhs = rhs;
+        return fail(h, BES_ERR_CUDA, "solver kernel (U=%d, G=%d) cannot be resident with %d warps per block", v.U,
+                    v.G, wpb);
+    const int systems_per_cta = wpb / v.G;
+    const int needed = (count + systems_per_cta - 1) / systems_per_cta;
+    L->v = v;
     L->wpb = wpb;
     L->grid = std::max(1, std::min(needed, per_sm * h->sm_count));
     return BES_OK;
@@ -358,7 +354,7 @@ bes_status enqueue_solve(bes_solver* h, DeviceProblem P, cudaStream_t s, const C
         Pc.work_counter = h->d_work + cls;
         cudaStream_t cs = h->class_stream[cls];
         CUDA_TRY(h, cudaStreamWaitEvent(cs, h->fork_ev, 0));
-        CUDA_TRY(h, bes::launch(L[cls].U, L[cls].rhs, Pc, L[cls].grid, L[cls].wpb, cs));
+        CUDA_TRY(h, bes::launch(L[cls].v, Pc, L[cls].grid, L[cls].wpb, cs));
         CUDA_TRY(h, cudaEventRecord(h->join_ev[cls], cs));
         CUDA_TRY(h, cudaStreamWaitEvent(s, h->join_ev[cls], 0));
         (*launches)++;
@@ -652,6 +648,11 @@ bes_status bes_solver_option(bes_solver* h, int32_t option, double value) {
             break;
         case BES_OPT_WARPS_PER_BLOCK: h->warps_per_block = (int)value; break;
         case BES_OPT_USE_CUDA_GRAPH: h->use_graph = value != 0.0; break;
+        case BES_OPT_WARPS_PER_SYSTEM:
+            if (!(value == 0.0 || value == 1.0))
+                return fail(h, BES_ERR_ARGUMENT, "SolverOption: WarpsPerSystem must be 0 (automatic) or 1");
+            h->warps_per_system = (int)value;
+            break;
         default:
             return fail(h, BES_ERR_OPTION, "SolverOption: option %d needs an index argument or is not applicable", option);
     }

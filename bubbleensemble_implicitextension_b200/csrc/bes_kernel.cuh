@@ -1,10 +1,12 @@
 /*
  * bes_kernel.cuh -- the persistent ensemble integrator for sm_100a.
  *
- * One warp integrates one system; lane l owns units l, l+32, ..., l+32(U-1)
- * (U = 1, 2, 4 for N <= 32, 64, 128).  Warps pull systems from a global work
- * counter until the ensemble is done, and each system runs `n_periods`
- * consecutive reference Solve() calls inside the one launch.
+ * A group of G warps integrates one system; lane l of warp w owns units
+ * 32 (G m + w) + l for m < U, so the system holds up to 32 U G units (single
+ * warps with U = 1, 2, 4, or U = 1 with G = 2, 4 warps for N <= 64, 128).
+ * Groups pull systems from a global work counter until the ensemble is done,
+ * and each system runs `n_periods` consecutive reference Solve() calls inside
+ * the one launch.
  *
  * Reference behaviour restated here (file:line in the reference):
  *   step loop, callbacks, write-back  SourceCodes/CoupledSystmes_PerBlock_Solver.cuh:82-648
@@ -21,12 +23,13 @@
  * transposed product A^T p~, which the reference forms with N block-wide
  * reductions per BiCG iteration, becomes one column tree per lane over the
  * operator W_ij = (rD_i C_ij) X0_j^2 that is formed once per right-hand side
- * in shared memory (leading dimension 32U+1: conflict-free row and column
- * reads).  Every scalar of the step control is warp-uniform and held in
- * registers, so a step needs no block barrier at all.
+ * in shared memory (leading dimension 32UG+1: conflict-free row and column
+ * reads).  Every scalar of the step control is uniform over the group and
+ * held in registers; a single-warp system needs no block barrier at all, a
+ * multi-warp system one named barrier per reduction.
  *
  * Arithmetic order (identical in the CPU oracle): sums over units are the
- * halving tree over units padded with zeros to 32U; the row products use
+ * halving tree over units padded with zeros to 32UG; the row products use
  * four interleaved fma chains over the columns (j mod 4) combined as
  * (s0 + s1) + (s2 + s3); every fused multiply-add is explicit (the file is
  * compiled with --fmad=false).
@@ -64,37 +67,41 @@ constexpr int NSAa = NSA > 0 ? NSA : 1;
 constexpr int NISAa = NISA > 0 ? NISA : 1;
 constexpr unsigned FULL = 0xffffffffu;
 
-/* Shared-memory doubles per warp for U units per lane: one NMAX x (NMAX+1)
- * matrix region (the operator W with the shared-memory operator, the system's
- * coupling matrix C with the register-resident operator), six broadcast
- * vectors and the system-scope arrays. */
-template <int U>
+/* Shared-memory doubles per system (G warps, U units per lane, NMAX = 32 U G
+ * units): one NMAX x (NMAX+1) matrix region (the operator W with the
+ * shared-memory operator, the system's coupling matrix C with the
+ * register-resident operator), six broadcast vectors, the group's exchange
+ * buffers (G > 1), the system-scope arrays and (U = G = 1 only) the unit
+ * parameters of the register-resident operator. */
+template <int U, int G = 1>
 struct WarpSmem {
-    static constexpr int NMAX = 32 * U;
+    static constexpr int NMAX = 32 * U * G;
     static constexpr int LDW = NMAX + 1;
     static constexpr int W_DOUBLES = NMAX * LDW;
     static constexpr int VEC_DOUBLES = 6 * NMAX;
-    static constexpr int SYS_DOUBLES = NSPa + NSAa + NISAa; /* ints stored in double slots */
-    static constexpr int UP_DOUBLES = NMAX * NUPa;          /* unit parameters, lane-contiguous */
-    /* per-warp stride rounded up to 256 bytes: every warp's vectors stay
+    static constexpr int XCH_DOUBLES = G > 1 ? 4 * NMAX : 0; /* two buffers of two values per unit */
+    static constexpr int SYS_DOUBLES = NSPa + NSAa + NISAa;  /* ints stored in double slots */
+    static constexpr int UP_DOUBLES = U == 1 && G == 1 ? NMAX * NUPa : 0; /* unit parameters, lane-contiguous */
+    /* per-system stride rounded up to 256 bytes: every system's vectors stay
      * 16-byte aligned for the double2 broadcast loads */
-    static constexpr int DOUBLES = (W_DOUBLES + VEC_DOUBLES + SYS_DOUBLES + UP_DOUBLES + 31) / 32 * 32;
+    static constexpr int DOUBLES = (W_DOUBLES + VEC_DOUBLES + XCH_DOUBLES + SYS_DOUBLES + UP_DOUBLES + 31) / 32 * 32;
     static constexpr int BYTES = DOUBLES * 8;
     static_assert(DOUBLES % 2 == 0 && W_DOUBLES % 2 == 0 && NMAX % 2 == 0,
                   "broadcast vectors must start on 16-byte boundaries");
 };
 
 /* Shared-memory layout of the shared-matrix variant (RHS = 3): one padded
- * copy of the launch's coupling matrix per CTA (leading dimension 32U+2:
+ * copy of the launch's coupling matrix per CTA (leading dimension NMAX+2:
  * rows are read lane-consecutive, each lane's column is 16-byte aligned and
- * its double2 reads are conflict-free), then per warp five broadcast vectors
- * and the system-scope arrays. */
-template <int U>
+ * its double2 reads are conflict-free), then per system five broadcast
+ * vectors, the group's exchange buffers and the system-scope arrays. */
+template <int U, int G = 1>
 struct SharedCSmem {
-    static constexpr int NMAX = 32 * U;
+    static constexpr int NMAX = 32 * U * G;
     static constexpr int LDC = NMAX + 2;
     static constexpr int C_DOUBLES = NMAX * LDC;
-    static constexpr int WARP_DOUBLES = (5 * NMAX + NSPa + NSAa + NISAa + 31) / 32 * 32;
+    static constexpr int XCH_DOUBLES = G > 1 ? 4 * NMAX : 0;
+    static constexpr int WARP_DOUBLES = (5 * NMAX + XCH_DOUBLES + NSPa + NSAa + NISAa + 31) / 32 * 32;
     static constexpr int C_BYTES = C_DOUBLES * 8;
     static constexpr int WARP_BYTES = WARP_DOUBLES * 8;
     static_assert(LDC % 2 == 0 && C_DOUBLES % 2 == 0 && WARP_DOUBLES % 2 == 0, "16-byte alignment");
@@ -174,53 +181,182 @@ __device__ __forceinline__ double warp_min(double s) {
     return s;
 }
 
-/* per-warp view of one system */
-template <int U>
+/* one warp's view of its system: the system runs on G warps (wis = this
+ * warp's index among them); slot m of lane l is unit 32 (G m + wis) + l */
+template <int U, int G = 1>
 struct Sys {
-    int lane, sid, N;
+    int lane, sid, N, wis;
+    unsigned bar;      /* named barrier of the system's G warps (G > 1) */
     int64_t off, tot;
     const double* C;   /* the system's coupling matrix in HBM */
     double* W;         /* matrix region in shared memory: W, or a padded copy of C */
     double *vp, *vpt, *vcpt, *vx1, *vxu, *vrd;
     double* upsh;      /* unit parameters of the register-operator variant: unit i at upsh[i * NUP] */
+    double* xch;       /* the group's exchange buffers (G > 1) */
+    mutable int xsel;  /* which exchange buffer the next group exchange uses */
     double* sPAR;
     double* sACC;
     int* isACC;
     double* gPAR;
     int* igPAR;
+    __device__ __forceinline__ int unit(int m) const { return 32 * (G * m + wis) + lane; }
 };
+
+/* ---------------------------------------------------------------------------
+ * Group primitives: with G = 1 they are the warp's own shuffles and votes;
+ * with G > 1 each call writes this warp's values into one of two exchange
+ * buffers, crosses one named barrier and reads every warp's values back (the
+ * two buffers alternate, so a buffer is rewritten only after a later barrier
+ * that every reader of its previous contents has passed).  All G warps of a
+ * system make the same sequence of calls: their control flow is identical
+ * because every decision comes out of these reductions. */
+template <int U, int G>
+__device__ __forceinline__ void grp_sync(const Sys<U, G>& S) {
+    if constexpr (G == 1) __syncwarp();
+    else asm volatile("bar.sync %0, %1;" ::"r"(S.bar), "r"(32 * G) : "memory");
+}
+
+template <int U, int G>
+__device__ __forceinline__ double* grp_buffer(const Sys<U, G>& S) {
+    double* b = S.xch + (S.xsel & 1) * (2 * 32 * U * G);
+    S.xsel++;
+    return b;
+}
+
+/* a[k][b]: value k of this lane's unit in block b = G m + wis, for all U G blocks */
+template <int U, int G, int K>
+__device__ __forceinline__ void grp_gather(const Sys<U, G>& S, const double (&v)[K][U], double (&a)[K][U * G]) {
+    if constexpr (G == 1) {
+#pragma unroll
+        for (int k = 0; k < K; k++)
+#pragma unroll
+            for (int m = 0; m < U; m++) a[k][m] = v[k][m];
+    } else {
+        double* buf = grp_buffer(S);
+#pragma unroll
+        for (int k = 0; k < K; k++)
+#pragma unroll
+            for (int m = 0; m < U; m++) buf[k * 32 * U * G + (G * m + S.wis) * 32 + S.lane] = v[k][m];
+        grp_sync(S);
+#pragma unroll
+        for (int k = 0; k < K; k++)
+#pragma unroll
+            for (int b = 0; b < U * G; b++) a[k][b] = buf[k * 32 * U * G + b * 32 + S.lane];
+    }
+}
+
+/* Sum over all units of the system in halving-tree order (blocks of 32 first,
+ * then the lanes); every lane of every warp of the system gets it. */
+template <int U, int G>
+__device__ __forceinline__ double grp_tree_sum(const Sys<U, G>& S, const double (&v)[U]) {
+    double in[1][U], a[1][U * G];
+#pragma unroll
+    for (int m = 0; m < U; m++) in[0][m] = v[m];
+    grp_gather<U, G, 1>(S, in, a);
+    return warp_tree_sum<U * G>(a[0]);
+}
+
+template <int U, int G>
+__device__ __forceinline__ double grp_tree_max(const Sys<U, G>& S, const double (&v)[U]) {
+    double in[1][U], a[1][U * G];
+#pragma unroll
+    for (int m = 0; m < U; m++) in[0][m] = v[m];
+    grp_gather<U, G, 1>(S, in, a);
+    return warp_tree_max<U * G>(a[0]);
+}
+
+template <int U, int G>
+__device__ __forceinline__ void grp_tree_max_sum(const Sys<U, G>& S, const double (&x)[U], const double (&y)[U],
+                                                 double& xmax, double& ysum) {
+    double in[2][U], a[2][U * G];
+#pragma unroll
+    for (int m = 0; m < U; m++) { in[0][m] = x[m]; in[1][m] = y[m]; }
+    grp_gather<U, G, 2>(S, in, a);
+    warp_tree_max_sum<U * G>(a[0], a[1], xmax, ysum);
+}
+
+/* one warp-uniform value per warp to all G warps: out[w] */
+template <int U, int G>
+__device__ __forceinline__ void grp_share(const Sys<U, G>& S, double v, double (&out)[G]) {
+    if constexpr (G == 1) {
+        out[0] = v;
+    } else {
+        double* buf = grp_buffer(S);
+        if (S.lane == 0) buf[S.wis] = v;
+        grp_sync(S);
+#pragma unroll
+        for (int w = 0; w < G; w++) out[w] = buf[w];
+    }
+}
+
+template <int U, int G>
+__device__ __forceinline__ double grp_min(const Sys<U, G>& S, double s) {
+    s = warp_min(s);
+    double w[G];
+    grp_share(S, s, w);
+#pragma unroll
+    for (int k = 1; k < G; k++) w[0] = fmin(w[0], w[k]);
+    return w[0];
+}
+
+template <int U, int G>
+__device__ __forceinline__ bool grp_all(const Sys<U, G>& S, bool p) {
+    double w[G];
+    grp_share(S, __all_sync(FULL, p) ? 1.0 : 0.0, w);
+    bool r = true;
+#pragma unroll
+    for (int k = 0; k < G; k++) r = r && w[k] != 0.0;
+    return r;
+}
+
+template <int U, int G>
+__device__ __forceinline__ bool grp_any(const Sys<U, G>& S, bool p) {
+    double w[G];
+    grp_share(S, __any_sync(FULL, p) ? 1.0 : 0.0, w);
+    bool r = false;
+#pragma unroll
+    for (int k = 0; k < G; k++) r = r || w[k] != 0.0;
+    return r;
+}
 
 /* A callback may change a system-scope scalar through its reference argument
  * (the reference's shared variables).  Units see the value from before the
- * callback round; afterwards the lowest unit that changed it wins. */
-__device__ __forceinline__ double resolve_shared(double before, double after_lane, int first_unit_lane) {
-    unsigned int key = (unsigned int)first_unit_lane;
-    unsigned int best = __reduce_min_sync(FULL, key);
-    if (best == 0xffffffffu) return before;
-    return __shfl_sync(FULL, after_lane, (int)(best & 31u));
+ * callback round; afterwards the lowest unit that changed it wins
+ * (first_unit: the lowest unit of this lane that changed it, or -1). */
+template <int U, int G>
+__device__ __forceinline__ double grp_resolve(const Sys<U, G>& S, double before, double after_lane, int first_unit) {
+    const unsigned int best = __reduce_min_sync(FULL, (unsigned int)first_unit);
+    const double val = __shfl_sync(FULL, after_lane, (int)(best & 31u));
+    double keys[G], vals[G];
+    grp_share(S, (double)best, keys);
+    grp_share(S, val, vals);
+    double kmin = keys[0], v = vals[0];
+#pragma unroll
+    for (int w = 1; w < G; w++)
+        if (keys[w] < kmin) { kmin = keys[w]; v = vals[w]; }
+    return kmin == 4294967295.0 ? before : v;
 }
-__device__ __forceinline__ int resolve_shared_int(int before, int after_lane, int first_unit_lane) {
-    unsigned int key = (unsigned int)first_unit_lane;
-    unsigned int best = __reduce_min_sync(FULL, key);
-    if (best == 0xffffffffu) return before;
-    return __shfl_sync(FULL, after_lane, (int)(best & 31u));
+
+template <int U, int G>
+__device__ __forceinline__ int grp_resolve_int(const Sys<U, G>& S, int before, int after_lane, int first_unit) {
+    return (int)grp_resolve<U, G>(S, (double)before, (double)after_lane, first_unit);
 }
 
 /* ---------------------------------------------------------------------------
  * Coupled right-hand side of the whole system (Steppers.cuh:432-562). */
-template <int U>
-__device__ __forceinline__ int coupled_rhs(const Sys<U>& S, const DeviceProblem& P, double T,
+template <int U, int G>
+__device__ __forceinline__ int coupled_rhs(const Sys<U, G>& S, const DeviceProblem& P, double T,
                                            double (&Xs)[U][UD], double (&F)[U][UD],
                                            double (&up)[U][NUPa], double (&ua)[U][NUAa],
                                            int (&iua)[U][NIUAa], bool& capped) {
-    constexpr int NMAX = WarpSmem<U>::NMAX;
-    constexpr int LDW = WarpSmem<U>::LDW;
+    constexpr int NMAX = WarpSmem<U, G>::NMAX;
+    constexpr int LDW = WarpSmem<U, G>::LDW;
     const int N = S.N;
     double xu[U], rd[U], r[U], rt[U], x[U], p[U], pt[U];
-    __syncwarp();
+    grp_sync(S);
 #pragma unroll
     for (int m = 0; m < U; m++) {
-        const int i = S.lane + 32 * m;
+        const int i = S.unit(m);
         if (i < N) {
             double Fl[UD], cpt, cpf;
             CoupledSystems_PerBlock_OdeFunction<double>(S.sid, i, Fl, Xs[m], T, up[m], S.sPAR, S.gPAR, S.igPAR,
@@ -239,11 +375,11 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U>& S, const DeviceProblem&
             rd[m] = 0.0;
         }
     }
-    __syncwarp();
+    grp_sync(S);
     /* b = rD (C CPT) + x_u, r = b - A x_u, W_ij = (rD_i C_ij) X1sq_j */
 #pragma unroll
     for (int m = 0; m < U; m++) {
-        const int i = S.lane + 32 * m;
+        const int i = S.unit(m);
         if (i < N) {
             double b0 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0, a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
             const double* Ci = S.C + i;
@@ -281,7 +417,7 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U>& S, const DeviceProblem&
     double prod[U];
 #pragma unroll
     for (int m = 0; m < U; m++) prod[m] = r[m] * rt[m];
-    double rho1 = warp_tree_sum<U>(prod);
+    double rho1 = grp_tree_sum<U, G>(S, prod);
     double rho2 = 0.0;
     int done = 0;
     bool exited = false;
@@ -298,18 +434,18 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U>& S, const DeviceProblem&
                 pt[m] = fma(beta, pt[m], rt[m]);
             }
         }
-        __syncwarp();
+        grp_sync(S);
 #pragma unroll
         for (int m = 0; m < U; m++) {
-            const int i = S.lane + 32 * m;
+            const int i = S.unit(m);
             S.vp[i] = p[m];
             S.vpt[i] = pt[m];
         }
-        __syncwarp();
+        grp_sync(S);
         double q[U], qt[U];
 #pragma unroll
         for (int m = 0; m < U; m++) {
-            const int i = S.lane + 32 * m;
+            const int i = S.unit(m);
             if (i < N) {
                 double q0 = 0.0, q1 = 0.0, q2 = 0.0, q3 = 0.0;
                 const double* Wi = S.W + i;
@@ -335,7 +471,7 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U>& S, const DeviceProblem&
         }
 #pragma unroll
         for (int m = 0; m < U; m++) prod[m] = pt[m] * q[m];
-        double alpha = rho1 / warp_tree_sum<U>(prod);
+        double alpha = rho1 / grp_tree_sum<U, G>(S, prod);
         double ar[U];
 #pragma unroll
         for (int m = 0; m < U; m++) {
@@ -347,7 +483,7 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U>& S, const DeviceProblem&
 #pragma unroll
         for (int m = 0; m < U; m++) prod[m] = r[m] * rt[m];
         double rmax, rho_next;
-        warp_tree_max_sum<U>(ar, prod, rmax, rho_next);
+        grp_tree_max_sum<U, G>(S, ar, prod, rmax, rho_next);
         rho2 = rho1;
         done++;
         if (rmax < 1e-6) { exited = true; break; }
@@ -481,26 +617,26 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
 
 /* ---------------------------------------------------------------------------
  * Coupled right-hand side with the launch's shared coupling matrix staged once
- * per CTA (RHS = 3, U = 2 or 4).  The products apply C to scaled vectors,
+ * per CTA (RHS = 3, 64 or 128 units).  The products apply C to scaled vectors,
  *   A x0 = rD (C (X1sq x0)),  A p = p + rD (C (X1sq p)),
  *   A^T p~ = p~ + X1sq (C^T (rD p~)),
  * with C row sums as four interleaved fma chains and C column sums in the
- * halving-tree order over 32U; the oracle's shared-matrix association
+ * halving-tree order over 32UG; the oracle's shared-matrix association
  * computes the same. */
-template <int U>
-__device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U>& S, const DeviceProblem& P, double T,
+template <int U, int G>
+__device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const DeviceProblem& P, double T,
                                                    double (&Xs)[U][UD], double (&F)[U][UD],
                                                    double (&up)[U][NUPa], double (&ua)[U][NUAa],
                                                    int (&iua)[U][NIUAa], bool& capped) {
-    constexpr int NMAX = SharedCSmem<U>::NMAX;
-    constexpr int LDC = SharedCSmem<U>::LDC;
+    constexpr int NMAX = SharedCSmem<U, G>::NMAX;
+    constexpr int LDC = SharedCSmem<U, G>::LDC;
     constexpr int H = NMAX / 2;
     const int N = S.N;
     double xu[U], rd[U], x1[U], r[U], rt[U], x[U], p[U], pt[U];
-    __syncwarp();
+    grp_sync(S);
 #pragma unroll
     for (int m = 0; m < U; m++) {
-        const int i = S.lane + 32 * m;
+        const int i = S.unit(m);
         if (i < N) {
             double Fl[UD], cpt, cpf;
             CoupledSystems_PerBlock_OdeFunction<double>(S.sid, i, Fl, Xs[m], T, up[m], S.sPAR, S.gPAR, S.igPAR,
@@ -522,7 +658,7 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U>& S, const Device
             S.vp[i] = 0.0;
         }
     }
-    __syncwarp();
+    grp_sync(S);
     const double2* cpt2 = reinterpret_cast<const double2*>(S.vcpt);
     const double2* z2 = reinterpret_cast<const double2*>(S.vp);
     const double2* zt2 = reinterpret_cast<const double2*>(S.vpt);
@@ -536,7 +672,7 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U>& S, const Device
             const double2 va = v2[j / 2], vb = v2[j / 2 + 1];
 #pragma unroll
             for (int m = 0; m < U; m++) {
-                const double* Crow = S.W + S.lane + 32 * m;
+                const double* Crow = S.W + S.unit(m);
                 if (j < N) a0[m] = fma(Crow[j * LDC], va.x, a0[m]);
                 if (j + 1 < N) a1[m] = fma(Crow[(j + 1) * LDC], va.y, a1[m]);
                 if (j + 2 < N) a2[m] = fma(Crow[(j + 2) * LDC], vb.x, a2[m]);
@@ -551,7 +687,7 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U>& S, const Device
     row_sums(z2, asum);
 #pragma unroll
     for (int m = 0; m < U; m++) {
-        if (S.lane + 32 * m < N) {
+        if (S.unit(m) < N) {
             const double b = fma(rd[m], bsum[m], xu[m]);
             const double ax = fma(rd[m], asum[m], xu[m]);
             r[m] = b - ax;
@@ -566,7 +702,7 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U>& S, const Device
     double prod[U];
 #pragma unroll
     for (int m = 0; m < U; m++) prod[m] = r[m] * rt[m];
-    double rho1 = warp_tree_sum<U>(prod);
+    double rho1 = grp_tree_sum<U, G>(S, prod);
     double rho2 = 0.0;
     int done = 0;
     bool exited = false;
@@ -583,20 +719,20 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U>& S, const Device
                 pt[m] = fma(beta, pt[m], rt[m]);
             }
         }
-        __syncwarp();
+        grp_sync(S);
 #pragma unroll
         for (int m = 0; m < U; m++) {
-            const int i = S.lane + 32 * m;
+            const int i = S.unit(m);
             S.vp[i] = x1[m] * p[m];    /* z  = X1sq p  */
             S.vpt[i] = rd[m] * pt[m];  /* z~ = rD p~   */
         }
-        __syncwarp();
+        grp_sync(S);
         double qs[U], qts[U];
         row_sums(z2, qs);
 #pragma unroll
         for (int m = 0; m < U; m++) {
             /* column i_m of C against z~: the first tree levels on the loads, then the halving tree over 32 */
-            const double2* Ccol2 = reinterpret_cast<const double2*>(S.W + (S.lane + 32 * m) * LDC);
+            const double2* Ccol2 = reinterpret_cast<const double2*>(S.W + (S.unit(m)) * LDC);
             double u[32];
 #pragma unroll
             for (int k = 0; k < 32; k += 2) {
@@ -623,13 +759,13 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U>& S, const Device
         double q[U], qt[U];
 #pragma unroll
         for (int m = 0; m < U; m++) {
-            const bool v = S.lane + 32 * m < N;
+            const bool v = S.unit(m) < N;
             q[m] = v ? fma(rd[m], qs[m], p[m]) : 0.0;
             qt[m] = v ? fma(x1[m], qts[m], pt[m]) : 0.0;
         }
 #pragma unroll
         for (int m = 0; m < U; m++) prod[m] = pt[m] * q[m];
-        const double alpha = rho1 / warp_tree_sum<U>(prod);
+        const double alpha = rho1 / grp_tree_sum<U, G>(S, prod);
         double ar[U];
 #pragma unroll
         for (int m = 0; m < U; m++) {
@@ -640,7 +776,7 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U>& S, const Device
             prod[m] = r[m] * rt[m];
         }
         double rmax, rho_next;
-        warp_tree_max_sum<U>(ar, prod, rmax, rho_next);
+        grp_tree_max_sum<U, G>(S, ar, prod, rmax, rho_next);
         rho2 = rho1;
         done++;
         if (rmax < 1e-6) { exited = true; break; }
@@ -653,14 +789,14 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U>& S, const Device
 }
 
 /* the right-hand side a kernel variant uses */
-template <int U, int RHS>
-__device__ __forceinline__ int rhs_eval(const Sys<U>& S, const DeviceProblem& P, double T, double (&Xs)[U][UD],
+template <int U, int RHS, int G>
+__device__ __forceinline__ int rhs_eval(const Sys<U, G>& S, const DeviceProblem& P, double T, double (&Xs)[U][UD],
                                         double (&F)[U][UD], double (&up)[U][NUPa], double (&ua)[U][NUAa],
                                         int (&iua)[U][NIUAa], bool& capped) {
     if constexpr (RHS == 0) {
-        return coupled_rhs<U>(S, P, T, Xs, F, up, ua, iua, capped);
+        return coupled_rhs<U, G>(S, P, T, Xs, F, up, ua, iua, capped);
     } else if constexpr (RHS == 3) {
-        return coupled_rhs_sharedc<U>(S, P, T, Xs, F, up, ua, iua, capped);
+        return coupled_rhs_sharedc<U, G>(S, P, T, Xs, F, up, ua, iua, capped);
     } else {
         static_assert(U == 1, "the register-resident operator needs one unit per lane");
         return coupled_rhs_regw<RHS == 2 ? 32 : 0>(S, P, T, Xs, F, up, ua, iua, capped);
@@ -682,13 +818,13 @@ struct Counters {
     int status;
 };
 
-template <int U>
-__device__ __forceinline__ bool valid_unit(const Sys<U>& S, int m) { return S.lane + 32 * m < S.N; }
+template <int U, int G>
+__device__ __forceinline__ bool valid_unit(const Sys<U, G>& S, int m) { return S.unit(m) < S.N; }
 
 /* the parameter array a callback gets for slot m of this lane */
-template <int U, int RHS>
-__device__ __forceinline__ double* upar_of(const Sys<U>& S, Lane<U>& L, int m) {
-    if constexpr (RHS == 1 || RHS == 2) return S.upsh + (S.lane + 32 * m) * NUPa;
+template <int U, int RHS, int G>
+__device__ __forceinline__ double* upar_of(const Sys<U, G>& S, Lane<U>& L, int m) {
+    if constexpr (RHS == 1 || RHS == 2) return S.upsh + (S.unit(m)) * NUPa;
     else return L.up[m];
 }
 
@@ -710,8 +846,8 @@ __constant__ double kRK4_A[4] = {0.0, 0.5, 0.5, 1.0};
  * The six stages run as one loop so the coupled right-hand side is inlined
  * once; stage s evaluates at X + dt * (sum_j<s a_sj K_j) with the terms
  * accumulated in the reference's order (first a product, then fmas). */
-template <int U, int RHS>
-__device__ __forceinline__ bool step_rkck45(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L,
+template <int U, int RHS, int G>
+__device__ __forceinline__ bool step_rkck45(const Sys<U, G>& S, const DeviceProblem& P, Lane<U>& L,
                                             double T, double dt, double (&Yn)[U][UD], double (&E)[U][UD],
                                             Counters& cnt, bool& capped) {
     double K[6][U][UD];
@@ -744,7 +880,7 @@ __device__ __forceinline__ bool step_rkck45(const Sys<U>& S, const DeviceProblem
                     Xs[m][c] = fma(acc, dt, L.X[m][c]);
                 }
         }
-        cnt.bicg += rhs_eval<U, RHS>(S, P, Ts, Xs, F, L.up, L.ua, L.iua, capped);
+        cnt.bicg += rhs_eval<U, RHS, G>(S, P, Ts, Xs, F, L.up, L.ua, L.iua, capped);
 #pragma unroll
         for (int j = 0; j < 6; j++)
 #pragma unroll
@@ -772,13 +908,13 @@ __device__ __forceinline__ bool step_rkck45(const Sys<U>& S, const DeviceProblem
             E[m][c] = fma(dt, fabs(e), 1e-18);
             if (valid_unit(S, m) && (!isfinite(Yn[m][c]) || !isfinite(E[m][c]))) finite = false;
         }
-    return __all_sync(FULL, finite);
+    return grp_all<U, G>(S, finite);
 }
 
 /* classical RK4 step (the reference has only its fixed-step controller,
  * ErrorControllers.cuh:424-450) */
-template <int U, int RHS>
-__device__ __forceinline__ bool step_rk4(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L,
+template <int U, int RHS, int G>
+__device__ __forceinline__ bool step_rk4(const Sys<U, G>& S, const DeviceProblem& P, Lane<U>& L,
                                          double T, double dt, double (&Yn)[U][UD], Counters& cnt, bool& capped) {
     double K[4][U][UD];
 #pragma unroll
@@ -811,7 +947,7 @@ __device__ __forceinline__ bool step_rk4(const Sys<U>& S, const DeviceProblem& P
                     Xs[m][c] = st == 3 ? fma(kprev, dt, L.X[m][c]) : fma(kprev * kRK4_A[st], dt, L.X[m][c]);
                 }
         }
-        cnt.bicg += rhs_eval<U, RHS>(S, P, Ts, Xs, F, L.up, L.ua, L.iua, capped);
+        cnt.bicg += rhs_eval<U, RHS, G>(S, P, Ts, Xs, F, L.up, L.ua, L.iua, capped);
 #pragma unroll
         for (int j = 0; j < 4; j++)
 #pragma unroll
@@ -833,25 +969,25 @@ __device__ __forceinline__ bool step_rk4(const Sys<U>& S, const DeviceProblem& P
             Yn[m][c] = fma(s, dt, L.X[m][c]);
             if (valid_unit(S, m) && !isfinite(Yn[m][c])) finite = false;
         }
-    return __all_sync(FULL, finite);
+    return grp_all<U, G>(S, finite);
 }
 
 /* dense-output store (DenseOutput.cuh:312-361), bounds-checked at the slot */
-template <int U>
-__device__ __forceinline__ void store_dense(const Sys<U>& S, const DeviceProblem& P, const Lane<U>& L,
+template <int U, int G>
+__device__ __forceinline__ void store_dense(const Sys<U, G>& S, const DeviceProblem& P, const Lane<U>& L,
                                             int& idx, int update_do, int update, int& skipped,
                                             double& do_time, double T, double TD1) {
     if (update_do == 1 && idx < P.ndo) {
 #pragma unroll
         for (int m = 0; m < U; m++) {
-            const int i = S.lane + 32 * m;
+            const int i = S.unit(m);
             if (i < S.N) {
 #pragma unroll
                 for (int c = 0; c < UD; c++)
                     P.dense_state[(int64_t)idx * UD * S.tot + (int64_t)c * S.tot + S.off + i] = L.X[m][c];
             }
         }
-        if (S.lane == 0) P.dense_time[(int64_t)idx * P.n_systems + S.sid] = T;
+        if (S.lane == 0 && S.wis == 0) P.dense_time[(int64_t)idx * P.n_systems + S.sid] = T;
     }
     if (update_do == 1) {
         idx++;
@@ -863,8 +999,8 @@ __device__ __forceinline__ void store_dense(const Sys<U>& S, const DeviceProblem
 
 /* ---------------------------------------------------------------------------
  * One reference Solve() of one system (Solver.cuh:82-648). */
-template <int U, int RHS>
-__device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, Counters& cnt,
+template <int U, int RHS, int G>
+__device__ void run_period(const Sys<U, G>& S, const DeviceProblem& P, Lane<U>& L, Counters& cnt,
                            double (&TD)[2], double& T, int& do_idx) {
     const double TD1 = TD[1];
     double dt = P.dt0, newdt = P.dt0;
@@ -891,32 +1027,32 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
         int DOnewL = do_idx;
 #pragma unroll
         for (int m = 0; m < U; m++) {
-            const int i = S.lane + 32 * m;
+            const int i = S.unit(m);
             if (i < S.N) {
                 double Tu = Tl, dTu = dTl;
                 int DOu = DOl;
-                CoupledSystems_PerBlock_Initialization<double>(S.sid, i, DOu, Tu, dTu, TD, L.X[m], upar_of<U, RHS>(S, L, m), S.sPAR,
+                CoupledSystems_PerBlock_Initialization<double>(S.sid, i, DOu, Tu, dTu, TD, L.X[m], upar_of<U, RHS, G>(S, L, m), S.sPAR,
                                                                S.gPAR, S.igPAR, L.ua[m], L.iua[m], S.sACC, S.isACC);
                 if (firstT < 0 && Tu != Tl) { firstT = i; TnewL = Tu; }
                 if (firstD < 0 && dTu != dTl) { firstD = i; dTnewL = dTu; }
                 if (firstO < 0 && DOu != DOl) { firstO = i; DOnewL = DOu; }
             }
         }
-        T = resolve_shared(T, TnewL, firstT < 0 ? -1 : firstT);
-        dt = resolve_shared(dt, dTnewL, firstD < 0 ? -1 : firstD);
+        T = grp_resolve<U, G>(S, T, TnewL, firstT < 0 ? -1 : firstT);
+        dt = grp_resolve<U, G>(S, dt, dTnewL, firstD < 0 ? -1 : firstD);
         newdt = dt;
-        do_idx = resolve_shared_int(do_idx, DOnewL, firstO < 0 ? -1 : firstO);
+        do_idx = grp_resolve_int<U, G>(S, do_idx, DOnewL, firstO < 0 ? -1 : firstO);
     }
     /* first event values (Solver.cuh:283-305) */
     if (NE > 0) {
 #pragma unroll
         for (int m = 0; m < U; m++)
             if (valid_unit(S, m))
-                CoupledSystems_PerBlock_EventFunction<double>(S.sid, S.lane + 32 * m, L.ev_a[m], T, dt, TD, L.X[m],
-                                                              upar_of<U, RHS>(S, L, m), S.sPAR, S.gPAR, S.igPAR, L.ua[m], L.iua[m],
+                CoupledSystems_PerBlock_EventFunction<double>(S.sid, S.unit(m), L.ev_a[m], T, dt, TD, L.X[m],
+                                                              upar_of<U, RHS, G>(S, L, m), S.sPAR, S.gPAR, S.igPAR, L.ua[m], L.iua[m],
                                                               S.sACC, S.isACC);
     }
-    if (P.ndo > 0) store_dense<U>(S, P, L, do_idx, update_do, 1, skipped, do_time, T, TD1);
+    if (P.ndo > 0) store_dense<U, G>(S, P, L, do_idx, update_do, 1, skipped, do_time, T, TD1);
 
     long long attempted = 0;
     bool terminate = false;
@@ -930,7 +1066,7 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
         double Yn[U][UD], E[U][UD];
         bool finite;
         if (P.algorithm == 1) {
-            finite = step_rkck45<U, RHS>(S, P, L, T, dt, Yn, E, cnt, capped);
+            finite = step_rkck45<U, RHS, G>(S, P, L, T, dt, Yn, E, cnt, capped);
             /* ErrorController_RKCK45 (ErrorControllers.cuh:454-542) */
             double rr = 1e30;
             int ru = 1;
@@ -945,8 +1081,8 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
                     }
                 }
             }
-            update = __all_sync(FULL, ru) ? 1 : 0;
-            double relerr = warp_min(rr);
+            update = grp_all<U, G>(S, ru) ? 1 : 0;
+            double relerr = grp_min<U, G>(S, rr);
             double mult = update == 1 ? 0.8 * bes::math::pow(relerr, 1.0 / 5.0)
                                       : 0.8 * bes::math::pow(relerr, 1.0 / 4.0);
             if (!isfinite(mult)) finite = false;
@@ -964,19 +1100,19 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
             newdt = fmin(newdt, P.dtmax);
             newdt = fmax(newdt, P.dtmin);
         } else {
-            finite = step_rk4<U, RHS>(S, P, L, T, dt, Yn, cnt, capped);
+            finite = step_rk4<U, RHS, G>(S, P, L, T, dt, Yn, cnt, capped);
             if (!finite) { cnt.status |= BES_STATUS_NONFINITE; terminate = true; update = 0; }
             newdt = P.dt0;
         }
-        if (__any_sync(FULL, capped)) cnt.status |= BES_STATUS_BICG_CAP;
+        if (grp_any<U, G>(S, capped)) cnt.status |= BES_STATUS_BICG_CAP;
 
         if (!terminate && NE > 0) {
             /* next event values at the trial state (Solver.cuh:393-414) */
 #pragma unroll
             for (int m = 0; m < U; m++)
                 if (valid_unit(S, m))
-                    CoupledSystems_PerBlock_EventFunction<double>(S.sid, S.lane + 32 * m, L.ev_n[m], T + dt, newdt, TD,
-                                                                  Yn[m], upar_of<U, RHS>(S, L, m), S.sPAR, S.gPAR, S.igPAR, L.ua[m],
+                    CoupledSystems_PerBlock_EventFunction<double>(S.sid, S.unit(m), L.ev_n[m], T + dt, newdt, TD,
+                                                                  Yn[m], upar_of<U, RHS, G>(S, L, m), S.sPAR, S.gPAR, S.igPAR, L.ua[m],
                                                                   L.iua[m], S.sACC, S.isACC);
             if (update == 1) {
                 /* EventTimeStepControl (EventHandling.cuh:216-268) */
@@ -997,8 +1133,8 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
                         }
                     }
                 }
-                if (__any_sync(FULL, corrected)) {
-                    evdt = warp_min(evdt);
+                if (grp_any<U, G>(S, corrected)) {
+                    evdt = grp_min<U, G>(S, evdt);
                     if (evdt < P.dtmin) {
                         cnt.status |= BES_STATUS_EVENT_MISSED;
                     } else {
@@ -1023,21 +1159,21 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
                 double TnewL = T, dTnewL = dt;
 #pragma unroll
                 for (int m = 0; m < U; m++) {
-                    const int i = S.lane + 32 * m;
+                    const int i = S.unit(m);
                     if (i < S.N) {
                         double Tu = Tl, dTu = dTl;
                         int Uu = udt;
                         CoupledSystems_PerBlock_ActionAfterSuccessfulTimeStep<double>(
-                            S.sid, i, Uu, Tu, dTu, TD, L.X[m], upar_of<U, RHS>(S, L, m), S.sPAR, S.gPAR, S.igPAR, L.ua[m], L.iua[m],
+                            S.sid, i, Uu, Tu, dTu, TD, L.X[m], upar_of<U, RHS, G>(S, L, m), S.sPAR, S.gPAR, S.igPAR, L.ua[m], L.iua[m],
                             S.sACC, S.isACC);
                         if (firstT < 0 && Tu != Tl) { firstT = i; TnewL = Tu; }
                         if (firstD < 0 && dTu != dTl) { firstD = i; dTnewL = dTu; }
                         if (Uu != udt) anyU = 1;
                     }
                 }
-                T = resolve_shared(T, TnewL, firstT);
-                dt = resolve_shared(dt, dTnewL, firstD);
-                if (__any_sync(FULL, anyU)) udt = 1;
+                T = grp_resolve<U, G>(S, T, TnewL, firstT);
+                dt = grp_resolve<U, G>(S, dt, dTnewL, firstD);
+                if (grp_any<U, G>(S, anyU)) udt = 1;
             }
             if (NE > 0) {
                 /* ActionAfterEventDetection when an event lands within tolerance (Solver.cuh:465-495) */
@@ -1046,7 +1182,7 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
                 double TnewL = T, dTnewL = dt;
 #pragma unroll
                 for (int m = 0; m < U; m++) {
-                    const int i = S.lane + 32 * m;
+                    const int i = S.unit(m);
                     if (i < S.N) {
 #pragma unroll
                         for (int e = 0; e < NE; e++) {
@@ -1056,7 +1192,7 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
                                 double Tu = Tl, dTu = dTl;
                                 int Uu = udt;
                                 CoupledSystems_PerBlock_ActionAfterEventDetection<double>(
-                                    S.sid, i, e, Uu, Tu, dTu, TD, L.X[m], upar_of<U, RHS>(S, L, m), S.sPAR, S.gPAR, S.igPAR, L.ua[m],
+                                    S.sid, i, e, Uu, Tu, dTu, TD, L.X[m], upar_of<U, RHS, G>(S, L, m), S.sPAR, S.gPAR, S.igPAR, L.ua[m],
                                     L.iua[m], S.sACC, S.isACC);
                                 if (firstT < 0 && Tu != Tl) { firstT = i; TnewL = Tu; }
                                 if (firstD < 0 && dTu != dTl) { firstD = i; dTnewL = dTu; }
@@ -1065,15 +1201,15 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
                         }
                     }
                 }
-                T = resolve_shared(T, TnewL, firstT);
-                dt = resolve_shared(dt, dTnewL, firstD);
-                if (__any_sync(FULL, anyU)) udt = 1;
+                T = grp_resolve<U, G>(S, T, TnewL, firstT);
+                dt = grp_resolve<U, G>(S, dt, dTnewL, firstD);
+                if (grp_any<U, G>(S, anyU)) udt = 1;
                 /* refresh event values at the accepted state (Solver.cuh:497-525) */
 #pragma unroll
                 for (int m = 0; m < U; m++)
                     if (valid_unit(S, m))
-                        CoupledSystems_PerBlock_EventFunction<double>(S.sid, S.lane + 32 * m, L.ev_a[m], T, newdt, TD,
-                                                                      L.X[m], upar_of<U, RHS>(S, L, m), S.sPAR, S.gPAR, S.igPAR,
+                        CoupledSystems_PerBlock_EventFunction<double>(S.sid, S.unit(m), L.ev_a[m], T, newdt, TD,
+                                                                      L.X[m], upar_of<U, RHS, G>(S, L, m), S.sPAR, S.gPAR, S.igPAR,
                                                                       L.ua[m], L.iua[m], S.sACC, S.isACC);
             }
         } else {
@@ -1087,7 +1223,7 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
             } else {
                 update_do = 0;
             }
-            store_dense<U>(S, P, L, do_idx, update_do, update, skipped, do_time, T, TD1);
+            store_dense<U, G>(S, P, L, do_idx, update_do, update, skipped, do_time, T, TD1);
         }
         if (update == 1 && (end == 1 || udt == 1)) terminate = true;
     }
@@ -1100,49 +1236,58 @@ __device__ void run_period(const Sys<U>& S, const DeviceProblem& P, Lane<U>& L, 
         int DOnewL = do_idx;
 #pragma unroll
         for (int m = 0; m < U; m++) {
-            const int i = S.lane + 32 * m;
+            const int i = S.unit(m);
             if (i < S.N) {
                 double Tu = Tl, dTu = dTl;
                 int DOu = DOl;
-                CoupledSystems_PerBlock_Finalization<double>(S.sid, i, DOu, Tu, dTu, TD, L.X[m], upar_of<U, RHS>(S, L, m), S.sPAR,
+                CoupledSystems_PerBlock_Finalization<double>(S.sid, i, DOu, Tu, dTu, TD, L.X[m], upar_of<U, RHS, G>(S, L, m), S.sPAR,
                                                              S.gPAR, S.igPAR, L.ua[m], L.iua[m], S.sACC, S.isACC);
                 if (firstT < 0 && Tu != Tl) { firstT = i; TnewL = Tu; }
                 if (firstD < 0 && dTu != dTl) { firstD = i; dTnewL = dTu; }
                 if (firstO < 0 && DOu != DOl) { firstO = i; DOnewL = DOu; }
             }
         }
-        T = resolve_shared(T, TnewL, firstT);
-        do_idx = resolve_shared_int(do_idx, DOnewL, firstO);
+        T = grp_resolve<U, G>(S, T, TnewL, firstT);
+        do_idx = grp_resolve_int<U, G>(S, do_idx, DOnewL, firstO);
     }
 }
 
 /* ---------------------------------------------------------------------------
- * The kernel: warps pull systems from the work counter.
- * RHS = 0: operator W in shared memory (any U); RHS = 1 / 2: operator in
- * registers (U = 1; 2 = every system of the launch has exactly 32 units);
+ * The kernel: groups of G warps pull systems from the work counter.
+ * RHS = 0: operator W in shared memory; RHS = 1 / 2: operator in registers
+ * (U = 1, G = 1; 2 = every system of the launch has exactly 32 units);
  * RHS = 3: every system of the launch shares one coupling matrix, staged once
- * per CTA (U = 2, 4; up to 8 warps per CTA). */
-template <int U, int RHS>
-__global__ void __launch_bounds__(RHS == 3 ? 256 : 128, 1) bes_ensemble_kernel(DeviceProblem P) {
+ * per CTA (up to 8 warps per CTA).  G > 1 runs one unit per lane (U = 1) and
+ * exchanges the group's values through shared memory and a named barrier per
+ * system slot (barrier 0 is left to __syncthreads). */
+template <int U, int RHS, int G>
+__global__ void __launch_bounds__(RHS == 3 || G > 1 ? 256 : 128, 1) bes_ensemble_kernel(DeviceProblem P) {
+    static_assert(G == 1 || U == 1, "multi-warp systems run one unit per lane");
+    static_assert(G == 1 || (RHS != 1 && RHS != 2), "the register-resident operator is single-warp");
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    Sys<U> S;
+    const int slot = wib / G;
+    Sys<U, G> S;
     S.lane = lane;
+    S.wis = wib % G;
+    S.bar = 1u + (unsigned)slot;
+    S.xsel = 0;
     S.tot = P.total_units;
     if constexpr (RHS == 3) {
         /* one copy of the launch's shared coupling matrix per CTA, zero-padded */
-        constexpr int LDC = SharedCSmem<U>::LDC;
+        using SM = SharedCSmem<U, G>;
+        constexpr int LDC = SM::LDC;
         const int s0 = P.order[0];
         const int n0 = P.units[s0];
         const double* Cg = P.coupling + P.coupling_offset[s0];
-        for (int idx = threadIdx.x; idx < SharedCSmem<U>::C_DOUBLES; idx += blockDim.x) {
+        for (int idx = threadIdx.x; idx < SM::C_DOUBLES; idx += blockDim.x) {
             const int r = idx % LDC, c = idx / LDC;
             smem[idx] = (r < n0 && c < n0) ? __ldg(Cg + r + (int64_t)c * n0) : 0.0;
         }
         __syncthreads();
-        constexpr int NM = SharedCSmem<U>::NMAX;
-        double* base = smem + SharedCSmem<U>::C_DOUBLES + (size_t)wib * SharedCSmem<U>::WARP_DOUBLES;
+        constexpr int NM = SM::NMAX;
+        double* base = smem + SM::C_DOUBLES + (size_t)slot * SM::WARP_DOUBLES;
         S.W = smem;
         S.vp = base;
         S.vpt = base + NM;
@@ -1150,30 +1295,40 @@ __global__ void __launch_bounds__(RHS == 3 ? 256 : 128, 1) bes_ensemble_kernel(D
         S.vx1 = base + 3 * NM;
         S.vxu = base + 4 * NM;
         S.vrd = nullptr;
-        S.sPAR = base + 5 * NM;
+        S.xch = base + 5 * NM;
+        S.sPAR = S.xch + SM::XCH_DOUBLES;
         S.upsh = nullptr;
     } else {
-        double* base = smem + (size_t)wib * WarpSmem<U>::DOUBLES;
+        using SM = WarpSmem<U, G>;
+        double* base = smem + (size_t)slot * SM::DOUBLES;
         S.W = base;
-        S.vp = base + WarpSmem<U>::W_DOUBLES;
-        S.vpt = S.vp + WarpSmem<U>::NMAX;
-        S.vcpt = S.vpt + WarpSmem<U>::NMAX;
-        S.vx1 = S.vcpt + WarpSmem<U>::NMAX;
-        S.vxu = S.vx1 + WarpSmem<U>::NMAX;
-        S.vrd = S.vxu + WarpSmem<U>::NMAX;
-        S.sPAR = S.vrd + WarpSmem<U>::NMAX;
-        S.upsh = S.sPAR + WarpSmem<U>::SYS_DOUBLES;
+        S.vp = base + SM::W_DOUBLES;
+        S.vpt = S.vp + SM::NMAX;
+        S.vcpt = S.vpt + SM::NMAX;
+        S.vx1 = S.vcpt + SM::NMAX;
+        S.vxu = S.vx1 + SM::NMAX;
+        S.vrd = S.vxu + SM::NMAX;
+        S.xch = S.vrd + SM::NMAX;
+        S.sPAR = S.xch + SM::XCH_DOUBLES;
+        S.upsh = S.sPAR + SM::SYS_DOUBLES;
     }
     S.sACC = S.sPAR + NSPa;
     S.isACC = reinterpret_cast<int*>(S.sACC + NSAa);
     S.gPAR = P.gpar;
     S.igPAR = P.igpar;
+    /* system-scope loads and stores are done by the group's first warp */
+    const bool leader = S.wis == 0;
 
     Lane<U> L;
     for (;;) {
         int k = 0;
-        if (lane == 0) k = atomicAdd(P.work_counter, 1);
+        if (lane == 0 && leader) k = atomicAdd(P.work_counter, 1);
         k = __shfl_sync(FULL, k, 0);
+        if constexpr (G > 1) {
+            double kk[G];
+            grp_share(S, (double)k, kk);
+            k = (int)kk[0];
+        }
         if (k >= P.n_active) break;
         const int sid = P.order ? P.order[k] : k;
         S.sid = sid;
@@ -1183,7 +1338,7 @@ __global__ void __launch_bounds__(RHS == 3 ? 256 : 128, 1) bes_ensemble_kernel(D
         /* unit-scope loads into registers / local memory (Solver.cuh:234-257) */
 #pragma unroll
         for (int m = 0; m < U; m++) {
-            const int i = lane + 32 * m;
+            const int i = S.unit(m);
             const bool v = i < S.N;
             const int64_t g = S.off + i;
 #pragma unroll
@@ -1199,9 +1354,11 @@ __global__ void __launch_bounds__(RHS == 3 ? 256 : 128, 1) bes_ensemble_kernel(D
             for (int c = 0; c < NIUA; c++) L.iua[m][c] = v ? P.iuacc[(int64_t)c * S.tot + g] : 0;
         }
         /* system-scope loads (Solver.cuh:82-130) */
-        for (int c = lane; c < NSP; c += 32) S.sPAR[c] = P.spar[(int64_t)c * P.n_systems + sid];
-        for (int c = lane; c < NSA; c += 32) S.sACC[c] = P.sacc[(int64_t)c * P.n_systems + sid];
-        for (int c = lane; c < NISA; c += 32) S.isACC[c] = P.isacc[(int64_t)c * P.n_systems + sid];
+        if (leader) {
+            for (int c = lane; c < NSP; c += 32) S.sPAR[c] = P.spar[(int64_t)c * P.n_systems + sid];
+            for (int c = lane; c < NSA; c += 32) S.sACC[c] = P.sacc[(int64_t)c * P.n_systems + sid];
+            for (int c = lane; c < NISA; c += 32) S.isACC[c] = P.isacc[(int64_t)c * P.n_systems + sid];
+        }
         if constexpr (RHS == 1 || RHS == 2) {
             /* stage the system's coupling matrix, zero-padded to 32 x 33 */
             constexpr int LDC = WarpSmem<1>::LDW;
@@ -1213,24 +1370,25 @@ __global__ void __launch_bounds__(RHS == 3 ? 256 : 128, 1) bes_ensemble_kernel(D
         double TD[2] = {P.time_domain[sid], P.time_domain[P.n_systems + sid]};
         double T = P.actual_time[sid];
         int do_idx = P.ndo > 0 ? P.dense_index[sid] : 0;
-        __syncwarp();
+        grp_sync(S);
         Counters cnt = {0ull, 0ull, 0ull, 0ull, 0};
         for (int per = 0; per < P.n_periods; per++) {
             if (per == P.reset_at) {
 #pragma unroll
                 for (int m = 0; m < U; m++) {
-                    for (int c = 0; c < NUA; c++) L.ua[m][c] = lane + 32 * m < S.N ? P.uacc_reset[c] : 0.0;
+                    const bool v = S.unit(m) < S.N;
+                    for (int c = 0; c < NUA; c++) L.ua[m][c] = v ? P.uacc_reset[c] : 0.0;
 #pragma unroll
-                    for (int c = 0; c < NIUA; c++) L.iua[m][c] = lane + 32 * m < S.N ? P.iuacc_reset[c] : 0;
+                    for (int c = 0; c < NIUA; c++) L.iua[m][c] = v ? P.iuacc_reset[c] : 0;
                 }
             }
-            run_period<U, RHS>(S, P, L, cnt, TD, T, do_idx);
+            run_period<U, RHS, G>(S, P, L, cnt, TD, T, do_idx);
         }
         /* write-back (Solver.cuh:599-648) */
-        __syncwarp();
+        grp_sync(S);
 #pragma unroll
         for (int m = 0; m < U; m++) {
-            const int i = lane + 32 * m;
+            const int i = S.unit(m);
             if (i < S.N) {
                 const int64_t g = S.off + i;
 #pragma unroll
@@ -1240,20 +1398,22 @@ __global__ void __launch_bounds__(RHS == 3 ? 256 : 128, 1) bes_ensemble_kernel(D
                 for (int c = 0; c < NIUA; c++) P.iuacc[(int64_t)c * S.tot + g] = L.iua[m][c];
             }
         }
-        for (int c = lane; c < NSA; c += 32) P.sacc[(int64_t)c * P.n_systems + sid] = S.sACC[c];
-        for (int c = lane; c < NISA; c += 32) P.isacc[(int64_t)c * P.n_systems + sid] = S.isACC[c];
-        if (lane == 0) {
-            P.actual_time[sid] = T;
-            P.time_domain[sid] = TD[0];
-            P.time_domain[P.n_systems + sid] = TD[1];
-            if (P.ndo > 0) P.dense_index[sid] = do_idx;
-            P.n_accepted[sid] += cnt.acc;
-            P.n_rejected[sid] += cnt.rej;
-            P.n_bicg_iter[sid] += cnt.bicg;
-            P.n_rhs[sid] += cnt.rhs;
-            P.status[sid] |= cnt.status;
+        if (leader) {
+            for (int c = lane; c < NSA; c += 32) P.sacc[(int64_t)c * P.n_systems + sid] = S.sACC[c];
+            for (int c = lane; c < NISA; c += 32) P.isacc[(int64_t)c * P.n_systems + sid] = S.isACC[c];
+            if (lane == 0) {
+                P.actual_time[sid] = T;
+                P.time_domain[sid] = TD[0];
+                P.time_domain[P.n_systems + sid] = TD[1];
+                if (P.ndo > 0) P.dense_index[sid] = do_idx;
+                P.n_accepted[sid] += cnt.acc;
+                P.n_rejected[sid] += cnt.rej;
+                P.n_bicg_iter[sid] += cnt.bicg;
+                P.n_rhs[sid] += cnt.rhs;
+                P.status[sid] |= cnt.status;
+            }
         }
-        __syncwarp();
+        grp_sync(S);
     }
 }
 

@@ -1,40 +1,93 @@
 /* bes_launch.cu -- dispatch from a run-time variant to the kernel instantiations. */
+#include <algorithm>
+
 #include "bes_kernel.cuh"
 #include "bes_launch.h"
 
 namespace bes {
 
-size_t warp_smem_bytes(int U) {
-    switch (U) {
-        case 1: return (size_t)WarpSmem<1>::BYTES;
-        case 2: return (size_t)WarpSmem<2>::BYTES;
-        default: return (size_t)WarpSmem<4>::BYTES;
+namespace {
+
+template <int U_, int RHS_, int G_>
+struct Tag {
+    static constexpr int U = U_, RHS = RHS_, G = G_;
+};
+
+/* calls f(Tag<U, RHS, G>{}) for the built variant v; false if v is not built */
+template <class F>
+bool dispatch(Variant v, F&& f) {
+    const int key = v.U * 100 + v.rhs * 10 + v.G;
+    switch (key) {
+        case 111: f(Tag<1, 1, 1>{}); return true;
+        case 121: f(Tag<1, 2, 1>{}); return true;
+        case 201: f(Tag<2, 0, 1>{}); return true;
+        case 231: f(Tag<2, 3, 1>{}); return true;
+        case 401: f(Tag<4, 0, 1>{}); return true;
+        case 431: f(Tag<4, 3, 1>{}); return true;
+        case 102: f(Tag<1, 0, 2>{}); return true;
+        case 132: f(Tag<1, 3, 2>{}); return true;
+        case 104: f(Tag<1, 0, 4>{}); return true;
+        case 134: f(Tag<1, 3, 4>{}); return true;
+        default: return false;
     }
 }
 
-size_t cta_smem_bytes(int U, int rhs, int warps) {
-    if (U == 1) return rhs == 2 ? cta_smem_t<1, 2>(warps) : cta_smem_t<1, 1>(warps);
-    if (U == 2) return rhs == 3 ? cta_smem_t<2, 3>(warps) : cta_smem_t<2, 0>(warps);
-    return rhs == 3 ? cta_smem_t<4, 3>(warps) : cta_smem_t<4, 0>(warps);
+}  // namespace
+
+bool variant_exists(Variant v) {
+    return dispatch(v, [](auto) {});
 }
 
-int max_warps_per_block(int U, int rhs) {
-    const int cap = rhs == 3 ? 8 : 4;   /* the kernels' launch bounds: 256 and 128 threads */
+size_t cta_smem_bytes(Variant v, int warps) {
+    size_t r = 0;
+    dispatch(v, [&](auto t) { using T = decltype(t); r = cta_smem_t<T::U, T::RHS, T::G>(warps); });
+    return r;
+}
+
+int max_warps_per_block(Variant v) {
+    /* the kernels' launch bounds: 256 threads with RHS 3 or G > 1, else 128 */
+    const int cap = (v.rhs == 3 || v.G > 1) ? 8 : 4;
     int w = 0;
-    while (w < cap && cta_smem_bytes(U, rhs, w + 1) <= 227 * 1024) w++;
+    while (w + v.G <= cap && cta_smem_bytes(v, w + v.G) <= 227 * 1024) w += v.G;
     return w;
 }
 
-cudaError_t occupancy(int U, int rhs, int warps, int* ctas_per_sm) {
-    if (U == 1) return rhs == 2 ? occupancy_t<1, 2>(warps, ctas_per_sm) : occupancy_t<1, 1>(warps, ctas_per_sm);
-    if (U == 2) return rhs == 3 ? occupancy_t<2, 3>(warps, ctas_per_sm) : occupancy_t<2, 0>(warps, ctas_per_sm);
-    return rhs == 3 ? occupancy_t<4, 3>(warps, ctas_per_sm) : occupancy_t<4, 0>(warps, ctas_per_sm);
+cudaError_t occupancy(Variant v, int warps, int* ctas_per_sm) {
+    cudaError_t e = cudaErrorInvalidValue;
+    dispatch(v, [&](auto t) { using T = decltype(t); e = occupancy_t<T::U, T::RHS, T::G>(warps, ctas_per_sm); });
+    return e;
 }
 
-cudaError_t launch(int U, int rhs, const DeviceProblem& P, int grid, int warps, cudaStream_t stream) {
-    if (U == 1) return rhs == 2 ? launch_t<1, 2>(P, grid, warps, stream) : launch_t<1, 1>(P, grid, warps, stream);
-    if (U == 2) return rhs == 3 ? launch_t<2, 3>(P, grid, warps, stream) : launch_t<2, 0>(P, grid, warps, stream);
-    return rhs == 3 ? launch_t<4, 3>(P, grid, warps, stream) : launch_t<4, 0>(P, grid, warps, stream);
+cudaError_t launch(Variant v, const DeviceProblem& P, int grid, int warps, cudaStream_t stream) {
+    cudaError_t e = cudaErrorInvalidValue;
+    dispatch(v, [&](auto t) { using T = decltype(t); e = launch_t<T::U, T::RHS, T::G>(P, grid, warps, stream); });
+    return e;
+}
+
+/* kernel variant of a units class: N <= 32 keeps the operator in registers
+ * (rhs 2: every system has exactly 32 units); larger N runs one unit per lane
+ * on 2 or 4 warps (or 2 or 4 units per lane on one warp) with W in shared
+ * memory, or one staged copy of a matrix shared by the whole class when the
+ * caller asked for shared coupling matrices (SharedCouplingMatrices). */
+Variant class_variant(int cls, bool all32, bool shared, int warps_per_system) {
+    if (cls == 0) return Variant{1, all32 ? 2 : 1, 1};
+    const int rhs = shared ? 3 : 0;
+    const int width = cls == 1 ? 2 : 4;
+    if (warps_per_system == 1) return Variant{width, rhs, 1};
+    return Variant{1, rhs, width};
+}
+
+/* CTA shape of a launch of `count` systems: spread small ensembles over every
+ * SM, fill SMs otherwise; `requested` > 0 asks for that many warps per CTA */
+int class_warps_per_block(Variant v, int count, int sm_count, int requested) {
+    const int cap = max_warps_per_block(v);
+    int wpb = requested;
+    if (wpb <= 0) {
+        const int systems = count <= sm_count ? 1 : (count <= 2 * sm_count ? 2 : cap / v.G);
+        wpb = systems * v.G;
+    }
+    wpb = std::max(v.G, std::min(wpb, cap)) / v.G * v.G;
+    return wpb;
 }
 
 }  // namespace bes

@@ -178,23 +178,19 @@ extern "C" bes_status bes_solve_periods_noalloc(const bes_noalloc_problem* p, in
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
     for (int cls = 0; cls < 3; cls++) {
         if (count[cls] == 0) continue;
-        const int U = cls == 0 ? 1 : (cls == 1 ? 2 : 4);
-        const int rhs = cls == 0 ? (all32 ? 2 : 1) : 0;
+        const bes::Variant v = bes::class_variant(cls, all32, false, 0);
         P.order = scratch + 4 + begin[cls];
         P.n_active = count[cls];
         P.work_counter = scratch + cls;
-        const int cap = bes::max_warps_per_block(U, rhs);
-        int wpb = p->warps_per_block > 0 ? p->warps_per_block
-                                          : (count[cls] <= sms ? 1 : (count[cls] <= 2 * sms ? 2 : cap));
-        wpb = wpb < 1 ? 1 : (wpb > cap ? cap : wpb);
+        const int wpb = bes::class_warps_per_block(v, count[cls], sms, p->warps_per_block);
         int per_sm = 0;
-        e = bes::occupancy(U, rhs, wpb, &per_sm);
+        e = bes::occupancy(v, wpb, &per_sm);
         if (e != cudaSuccess || per_sm < 1)
             return report(p, BES_ERR_CUDA, "bes_solve_periods_noalloc: kernel class %lld cannot be resident (cudaError %lld)",
                           (long long)cls, (long long)e);
-        const int needed = (count[cls] + wpb - 1) / wpb;
+        const int needed = (count[cls] + wpb / v.G - 1) / (wpb / v.G);
         const int grid = needed < per_sm * sms ? needed : per_sm * sms;
-        e = bes::launch(U, rhs, P, grid, wpb, st);
+        e = bes::launch(v, P, grid, wpb, st);
         if (e != cudaSuccess)
             return report(p, BES_ERR_CUDA, "bes_solve_periods_noalloc: launch of class %lld failed (cudaError %lld)",
                           (long long)cls, (long long)e);

@@ -69,6 +69,7 @@ class ListOfSolverOptions(IntEnum):
     BiCGMaxIterations = 101
     WarpsPerBlock = 102
     UseCudaGraph = 103
+    WarpsPerSystem = 104
 
 
 class Algorithms(IntEnum):

@@ -89,6 +89,9 @@ typedef int32_t bes_status;
 #define BES_OPT_WARPS_PER_BLOCK 102        /* launch shape: systems (warps) per CTA, 0 = automatic */
 #define BES_OPT_USE_CUDA_GRAPH 103         /* 1 (default): bes_solve_periods captures its launches once into a
                                               CUDA graph and replays it; 0: direct launches */
+#define BES_OPT_WARPS_PER_SYSTEM 104       /* 0 (default): systems of 33-64 units run on 2 warps and of 65-128
+                                              units on 4 warps (one unit per lane); 1: one warp per system
+                                              (2 or 4 units per lane).  Results are bit-identical. */
 
 /* Algorithms, Interface.cuh:33 */
 #define BES_RK4 0

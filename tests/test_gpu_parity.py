@@ -81,12 +81,47 @@ def test_graph_replay_equals_direct_launches(gpu):
     assert_bitwise(replay, direct, KEYS)
 
 
-@pytest.mark.parametrize("n,seed", [(128, 31), (100, 32), (64, 33), (48, 34)])
-def test_shared_matrix_staged_per_cta(n, seed, gpu, oracle_lib):
+@pytest.mark.parametrize("n,seed,wps,wpb", [(128, 31, 0, 8), (100, 32, 1, 4), (64, 33, 0, 8), (48, 34, 1, 4),
+                                            (72, 35, 0, 4), (40, 36, 0, 2)])
+def test_shared_matrix_staged_per_cta(n, seed, wps, wpb, gpu, oracle_lib):
     """SharedCouplingMatrices on: one matrix for the whole launch, staged once per
-    CTA; the products follow the oracle's shared-matrix association."""
+    CTA; the products follow the oracle's shared-matrix association (on 2 or 4
+    warps per system, or one warp with 2 or 4 units per lane)."""
     ens = bounded(W.c3_ensemble(n_systems=6, n_units=n, seed=seed, pa_bar=1.0, f_khz=150.0, n_periods=1,
                                 reset_at=-1, cube_um=400.0 * (n / 32) ** (1 / 3)))
-    got = run_gpu(ens, n_periods=1, reset_at=-1, shared_matrices=True, warps_per_block=4)
+    got = run_gpu(ens, n_periods=1, reset_at=-1, shared_matrices=True, warps_per_block=wpb, warps_per_system=wps)
     want = oracle_lib.run(ens, n_periods=1, reset_at=-1, shared_assoc=True)
     assert_bitwise(got, want, KEYS)
+
+
+def test_single_warp_systems_match_oracle(gpu, oracle_lib):
+    """WarpsPerSystem = 1: systems above 32 units on one warp (2 or 4 units per lane)."""
+    ens = bounded(ragged_ensemble([33, 64, 65, 128, 90, 47], seed=21))
+    got = run_gpu(ens, n_periods=1, reset_at=-1, warps_per_system=1)
+    want = oracle_lib.run(ens, n_periods=1, reset_at=-1)
+    assert_bitwise(got, want, KEYS)
+
+
+def test_multi_warp_dense_output_and_rk4(gpu, oracle_lib):
+    """Multi-warp systems with dense output (the group's first warp stores the
+    time) and with the RK4 stepper."""
+    ens = bounded(ragged_ensemble([40, 120], seed=23))
+    got = run_gpu(ens, n_periods=1, reset_at=-1, ndo=16, do_min_dt=0.05)
+    want = oracle_lib.run(ens, n_periods=1, reset_at=-1, ndo=16, do_min_dt=0.05)
+    assert_bitwise(got, want, KEYS + ["dense_index", "dense_time", "dense_state"])
+    ens.dt0 = 2e-3
+    got = run_gpu(ens, n_periods=1, reset_at=-1, algorithm=S.Algorithms.RK4)
+    want = oracle_lib.run(ens, n_periods=1, reset_at=-1, algorithm=0)
+    assert_bitwise(got, want, KEYS)
+
+
+def test_multi_warp_groups_pull_many_systems(gpu):
+    """Many more systems than resident groups, several groups per CTA: the
+    multi-warp and single-warp layouts give identical results."""
+    rng = np.random.default_rng(41)
+    ens = bounded(ragged_ensemble(list(rng.integers(33, 129, 700)), seed=42), budget=400)
+    a = run_gpu(ens, n_periods=1, reset_at=-1, warps_per_system=1)
+    b = run_gpu(ens, n_periods=1, reset_at=-1)
+    c = run_gpu(ens, n_periods=1, reset_at=-1, warps_per_block=2)
+    assert_bitwise(b, a, KEYS)
+    assert_bitwise(c, a, KEYS)
