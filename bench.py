@@ -84,6 +84,8 @@ def parse():
     ap.add_argument("--cpu-sample-systems", type=int, default=32)
     ap.add_argument("--systems", type=int, default=0,
                     help="profiling only: integrate an evenly strided subset of S systems (0: all)")
+    ap.add_argument("--warps-per-system", type=int, default=0, choices=[0, 1],
+                    help="0: systems above 32 units on 2 or 4 warps (default); 1: one warp per system")
     return ap.parse_args()
 
 
@@ -214,6 +216,8 @@ def run_b200(args, rank, world, local):
     # c2_period1; a system that needs more (the minimum-step cases) is cut short and counted
     ens.max_steps_per_period = 50_000
     ps = ens.make_solver(device=local)
+    if args.warps_per_system:
+        ps.SolverOption(S.ListOfSolverOptions.WarpsPerSystem, args.warps_per_system)
     stream = torch.cuda.current_stream(dev)
     ps.set_stream(stream.cuda_stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
@@ -306,7 +310,9 @@ def run_b200(args, rank, world, local):
         "config": {"workload": WORKLOADS[args.workload], "systems": ens.n_systems,
                    "units_per_system": int(ens.units[0]) if len(set(ens.units.tolist())) == 1 else "mixed",
                    "total_units": ens.total_units,
-                   "periods_per_step": 1, "l2": "flushed between timed steps (256 MiB write, untimed)",
+                   "periods_per_step": 1,
+                   "warps_per_system": "one" if args.warps_per_system else "2 or 4 above 32 units",
+                   "l2": "flushed between timed steps (256 MiB write, untimed)",
                    "parallelism": f"{world} independent ensemble replica(s), one per GPU"},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None,
