@@ -137,44 +137,6 @@ __device__ __forceinline__ double warp_tree_sum(const double (&v)[U]) {
     return s;
 }
 
-template <int U>
-__device__ __forceinline__ double warp_tree_max(const double (&v)[U]) {
-    double a[U];
-#pragma unroll
-    for (int m = 0; m < U; m++) a[m] = v[m];
-#pragma unroll
-    for (int h = U / 2; h >= 1; h /= 2)
-#pragma unroll
-        for (int m = 0; m < h; m++) a[m] = fmax(a[m], a[m + h]);
-    double s = a[0];
-#pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) s = fmax(s, __shfl_xor_sync(FULL, s, o));
-    return s;
-}
-
-/* max of a and halving-tree sum of b in one interleaved butterfly */
-template <int U>
-__device__ __forceinline__ void warp_tree_max_sum(const double (&a)[U], const double (&b)[U], double& amax,
-                                                  double& bsum) {
-    double x[U], y[U];
-#pragma unroll
-    for (int m = 0; m < U; m++) { x[m] = a[m]; y[m] = b[m]; }
-#pragma unroll
-    for (int h = U / 2; h >= 1; h /= 2)
-#pragma unroll
-        for (int m = 0; m < h; m++) { x[m] = fmax(x[m], x[m + h]); y[m] = y[m] + y[m + h]; }
-    double s = x[0], t = y[0];
-#pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) {
-        const double so = __shfl_xor_sync(FULL, s, o);
-        const double to = __shfl_xor_sync(FULL, t, o);
-        s = fmax(s, so);
-        t = t + to;
-    }
-    amax = s;
-    bsum = t;
-}
-
 __device__ __forceinline__ double warp_min(double s) {
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) s = fmin(s, __shfl_xor_sync(FULL, s, o));
@@ -256,23 +218,45 @@ __device__ __forceinline__ double grp_tree_sum(const Sys<U, G>& S, const double 
     return warp_tree_sum<U * G>(a[0]);
 }
 
+/* BiCG exit test and next rho in one exchange: returns whether the fmax-tree
+ * maximum of x over the system's units is below lim, and sets ysum to the
+ * halving-tree sum of y.  The fmax tree ignores NaN unless every value is
+ * NaN, so "max < lim" is exactly "every non-NaN value is below lim and at
+ * least one value is not NaN"; two warp votes decide it without a max tree. */
 template <int U, int G>
-__device__ __forceinline__ double grp_tree_max(const Sys<U, G>& S, const double (&v)[U]) {
-    double in[1][U], a[1][U * G];
+__device__ __forceinline__ bool grp_sum_max_below(const Sys<U, G>& S, const double (&x)[U], const double (&y)[U],
+                                                  double lim, double& ysum) {
+    bool ok = true, seen = false;
 #pragma unroll
-    for (int m = 0; m < U; m++) in[0][m] = v[m];
-    grp_gather<U, G, 1>(S, in, a);
-    return warp_tree_max<U * G>(a[0]);
-}
-
-template <int U, int G>
-__device__ __forceinline__ void grp_tree_max_sum(const Sys<U, G>& S, const double (&x)[U], const double (&y)[U],
-                                                 double& xmax, double& ysum) {
-    double in[2][U], a[2][U * G];
+    for (int m = 0; m < U; m++) {
+        ok = ok && (isnan(x[m]) || x[m] < lim);
+        seen = seen || !isnan(x[m]);
+    }
+    const bool wok = __all_sync(FULL, ok), wseen = __any_sync(FULL, seen);
+    if constexpr (G == 1) {
+        ysum = warp_tree_sum<U>(y);
+        return wok && wseen;
+    } else {
+        /* the sum's blocks and one flag word per warp share one exchange buffer */
+        double* buf = grp_buffer(S);
+        constexpr int NB = U * G;
 #pragma unroll
-    for (int m = 0; m < U; m++) { in[0][m] = x[m]; in[1][m] = y[m]; }
-    grp_gather<U, G, 2>(S, in, a);
-    warp_tree_max_sum<U * G>(a[0], a[1], xmax, ysum);
+        for (int m = 0; m < U; m++) buf[(G * m + S.wis) * 32 + S.lane] = y[m];
+        if (S.lane == 0) buf[32 * NB + S.wis] = (wok ? 1.0 : 0.0) + (wseen ? 2.0 : 0.0);
+        grp_sync(S);
+        double a[NB];
+#pragma unroll
+        for (int b = 0; b < NB; b++) a[b] = buf[b * 32 + S.lane];
+        ysum = warp_tree_sum<NB>(a);
+        bool all_ok = true, any_seen = false;
+#pragma unroll
+        for (int w = 0; w < G; w++) {
+            const double f = buf[32 * NB + w];
+            all_ok = all_ok && (f == 1.0 || f == 3.0);
+            any_seen = any_seen || f >= 2.0;
+        }
+        return all_ok && any_seen;
+    }
 }
 
 /* one warp-uniform value per warp to all G warps: out[w] */
@@ -482,11 +466,11 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U, G>& S, const DeviceProbl
         }
 #pragma unroll
         for (int m = 0; m < U; m++) prod[m] = r[m] * rt[m];
-        double rmax, rho_next;
-        grp_tree_max_sum<U, G>(S, ar, prod, rmax, rho_next);
+        double rho_next;
+        const bool small = grp_sum_max_below<U, G>(S, ar, prod, 1e-6, rho_next);
         rho2 = rho1;
         done++;
-        if (rmax < 1e-6) { exited = true; break; }
+        if (small) { exited = true; break; }
         rho1 = rho_next;
     }
     if (!exited) capped = true;
@@ -603,11 +587,11 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
         rt = fma(-alpha, qt, rt);
         double ar[1] = {fabs(r)};
         prod[0] = r * rt;
-        double rmax, rho_next;
-        warp_tree_max_sum<1>(ar, prod, rmax, rho_next);
+        double rho_next;
+        const bool small = grp_sum_max_below<1, 1>(S, ar, prod, 1e-6, rho_next);
         rho2 = rho1;
         done++;
-        if (rmax < 1e-6) { exited = true; break; }
+        if (small) { exited = true; break; }
         rho1 = rho_next;
     }
     if (!exited) capped = true;
@@ -775,11 +759,11 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const Dev
             ar[m] = fabs(r[m]);
             prod[m] = r[m] * rt[m];
         }
-        double rmax, rho_next;
-        grp_tree_max_sum<U, G>(S, ar, prod, rmax, rho_next);
+        double rho_next;
+        const bool small = grp_sum_max_below<U, G>(S, ar, prod, 1e-6, rho_next);
         rho2 = rho1;
         done++;
-        if (rmax < 1e-6) { exited = true; break; }
+        if (small) { exited = true; break; }
         rho1 = rho_next;
     }
     if (!exited) capped = true;
