@@ -60,6 +60,11 @@ WORKLOADS = {
     "c3_period1": ("c3_period1: 4096 systems sharing one N = 128 cloud (1 mm cube, R_E lognormal median 4 um sigma 0.4 "
                    "clipped to [1,12] um, seed 3), 200 kHz at 1.2 bar, initial radii perturbed by 1e-3 U(-1,1) per "
                    "bubble, RKCK45 rtol=atol=1e-10, FP64 BiCG; one step = one acoustic period of every system from rest"),
+    "c5_sweep": ("c5_sweep: the centre 128 x 128 window of the 1024 x 1024 amplitude (0.5-2 bar, linear) x frequency "
+                 "(20-200 kHz, log) grid of N = 32 line systems (d = 150 um, R_E ~ U(2,8) um seed 1), 8 periods with the "
+                 "first 4 discarded; plain solver on every point vs the surrogate-screened sweep (solver lattice every "
+                 "4th point, network corrected by the lattice residuals, disagreeing cells integrated, 2% audit); "
+                 "network trained first on 8192 solver runs with random amplitude, frequency and radius draws"),
 }
 
 
@@ -84,6 +89,12 @@ def parse():
     ap.add_argument("--cpu-sample-systems", type=int, default=32)
     ap.add_argument("--systems", type=int, default=0,
                     help="profiling only: integrate an evenly strided subset of S systems (0: all)")
+    ap.add_argument("--sweep-window", type=int, default=128, help="c5_sweep: window side within the 1024 grid")
+    ap.add_argument("--sweep-train", type=int, default=8192, help="c5_sweep: solver runs to train the network on")
+    ap.add_argument("--sweep-stride", type=int, default=4)
+    ap.add_argument("--sweep-spread", type=float, default=0.05)
+    ap.add_argument("--sweep-disagreement", type=float, default=0.02)
+    ap.add_argument("--sweep-dump", type=str, default="", help="c5_sweep: write the maps to this .npz")
     ap.add_argument("--warps-per-system", type=int, default=0, choices=[0, 1],
                     help="0: systems above 32 units on 2 or 4 warps (default); 1: one warp per system")
     return ap.parse_args()
@@ -374,10 +385,86 @@ def run_reference(args, rank, world):
     }
 
 
+def run_sweep(args, rank, world, local):
+    """Sweep time of the plain solver vs the surrogate-screened sweep, same GPU, same grid window."""
+    import torch
+
+    from bubbleensemble_implicitextension_b200 import surrogate as SG
+    from bubbleensemble_implicitextension_b200 import workloads as W
+
+    if rank != 0:
+        return None
+    torch.cuda.set_device(local)
+    n_grid, win, n_per, reset = 1024, args.sweep_window, 8, 4
+    pa_full = W.linspace_ref(0.5, 2.0, n_grid)
+    f_full = np.logspace(np.log10(20.0), np.log10(200.0), n_grid)
+    lo = (n_grid - win) // 2
+    pa, fr = pa_full[lo:lo + win], f_full[lo:lo + win]
+    radii = np.random.default_rng(1).uniform(2.0, 8.0, 32)
+
+    def solve(pa_pts, f_pts):
+        ens = SG.line_ensemble(pa_pts, f_pts, np.broadcast_to(radii, (len(pa_pts), 32)), n_periods=n_per,
+                               reset_at=reset)
+        return SG.solve_ensemble(ens)[0]
+
+    # the network: trained once on solver runs (reported, not part of either sweep's time)
+    t0 = time.perf_counter()
+    X, Y, status, gen_s = SG.generate_runs(args.sweep_train, seed=7, n_periods=n_per, reset_at=reset)
+    ok = (status & 4) == 0
+    net = SG.MLP(max_batch=4096, seed=2)
+    net.fit(X[ok], Y[ok], steps=3000, batch=512, lr=2e-3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    # plain sweep: every point
+    PA, FR = np.meshgrid(pa, fr, indexing="ij")
+    t0 = time.perf_counter()
+    plain = solve(PA.ravel(), FR.ravel()).reshape(win, win, 2)
+    plain_s = time.perf_counter() - t0
+    # screened sweep
+    res = SG.screen_sweep_lattice(net, pa, fr, radii, solve, stride=args.sweep_stride,
+                                  cell_spread=args.sweep_spread, cell_disagreement=args.sweep_disagreement)
+    net.close()
+    served = ~res.integrated
+    s_true = 10.0 ** plain[..., 0]
+    e_s = np.abs(10.0 ** res.map[..., 0] - s_true) / s_true
+    e_r = np.abs(res.map[..., 1] - plain[..., 1]) / np.maximum(np.abs(plain[..., 1]), 1e-12)
+    same = bool(np.array_equal(res.map[res.integrated], plain[res.integrated]))
+    if args.sweep_dump:
+        np.savez_compressed(args.sweep_dump, plain=plain, screened=res.map, integrated=res.integrated,
+                            lattice=res.lattice, audited=res.audited, pa=pa, fr=fr, radii=radii)
+
+    def q(e, p):
+        return float(np.quantile(e[served], p)) if served.any() else 0.0
+
+    return {
+        "metric": "sweep time vs plain at <=1% max relative map error", "value": plain_s / res.seconds, "unit": "x",
+        "higher_is_better": True, "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": 1e3 * res.seconds,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 solver, bf16/fp32 network", "data": DATA,
+        "config": {"workload": WORKLOADS["c5_sweep"], "points": win * win, "lattice_stride": args.sweep_stride,
+                   "cell_spread": args.sweep_spread, "cell_disagreement": args.sweep_disagreement,
+                   "audit_fraction": 0.02, "training_runs": int(args.sweep_train)},
+        "sweep": {"plain_s": plain_s, "screened_s": res.seconds, "screened_solver_s": res.solve_seconds,
+                  "integrated_fraction": float(res.integrated.mean()), "served_points": int(served.sum()),
+                  "served_strength_rel_error": {"max": q(e_s, 1.0), "p99": q(e_s, 0.99), "mean":
+                                                float(e_s[served].mean()) if served.any() else 0.0},
+                  "served_rmax_rel_error": {"max": q(e_r, 1.0), "p99": q(e_r, 0.99)},
+                  "meets_1pct_max_error": bool(q(e_s, 1.0) <= 0.01),
+                  "audit_max_rel_error": res.audit_max_rel_error,
+                  "integrated_points_equal_plain": same,
+                  "network_training_s": train_s, "training_data_solver_s": gen_s},
+        "gpu_launches": None,
+    }
+
+
 def main():
     args = parse()
     rank, world, local = dist_init(args.gpus)
-    line = run_reference(args, rank, world) if args.impl == "reference" else run_b200(args, rank, world, local)
+    if args.workload == "c5_sweep":
+        line = (run_sweep(args, rank, world, local) if args.impl == "b200" else
+                ({"impl": "reference", "unavailable": "the reference has no surrogate; the plain solver arm of the "
+                  "sweep is timed in the same line"} if rank == 0 else None))
+    else:
+        line = run_reference(args, rank, world) if args.impl == "reference" else run_b200(args, rank, world, local)
     if rank == 0 and line is not None:
         print(json.dumps(line), flush=True)
     if world > 1:

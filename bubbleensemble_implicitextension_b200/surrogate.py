@@ -15,6 +15,11 @@ maximum.  The training data come from the solver itself (:func:`generate_runs`).
 prediction changes steeply between grid neighbours plus a random audit
 sample, integrates only those with the solver, and serves the rest from the
 network; the audit measures the error of what the network served.
+:func:`screen_sweep_lattice` is the multi-fidelity form used by the sweep
+benchmark: the solver integrates a coarse lattice of the grid, the network's
+map is corrected by the bilinearly interpolated lattice residuals, and every
+lattice cell whose corners disagree, or where the corrected network departs
+from plain interpolation of the corners, is integrated in full.
 """
 from __future__ import annotations
 
@@ -265,3 +270,91 @@ def screen_sweep(mlp: MLP, pa: np.ndarray, f_khz: np.ndarray, radii_um: np.ndarr
         err = float(np.max(np.abs(pred[a_idx][:, 0] - sol) / np.maximum(np.abs(sol), 1e-3)))
     return ScreenResult(map=out, integrated=todo, audited=audit, audit_max_rel_error=err,
                         seconds=time.perf_counter() - t0)
+
+
+@dataclasses.dataclass
+class LatticeScreenResult:
+    map: np.ndarray            # served values [n_pa, n_f, 2]
+    integrated: np.ndarray     # bool [n_pa, n_f]: the solver's values (lattice, flagged cells, audit)
+    lattice: np.ndarray        # bool [n_pa, n_f]: lattice points
+    audited: np.ndarray        # bool [n_pa, n_f]: audit points outside flagged cells
+    audit_max_rel_error: float # corrected-network error on the audit points, collapse strength
+    solve_seconds: float       # time inside the solver (both passes)
+    seconds: float             # whole screened sweep
+
+
+def _lattice_axis(n: int, stride: int):
+    """Lattice indices of one grid axis (every stride-th point and the last one)
+    and, per grid point, its cell index and bilinear weight."""
+    idx = np.unique(np.r_[np.arange(0, n, stride), n - 1])
+    cell = np.clip(np.searchsorted(idx, np.arange(n), side="right") - 1, 0, len(idx) - 2)
+    t = (np.arange(n) - idx[cell]) / (idx[cell + 1] - idx[cell])
+    return idx, cell, t
+
+
+def screen_sweep_lattice(mlp: "MLP", pa: np.ndarray, f_khz: np.ndarray, radii_um: np.ndarray,
+                         solve: Callable[[np.ndarray, np.ndarray], np.ndarray], stride: int = 4,
+                         cell_spread: float = 0.05, cell_disagreement: float = 0.02,
+                         audit_fraction: float = 0.02, seed: int = 0) -> LatticeScreenResult:
+    """Multi-fidelity sweep: solver lattice + network corrected by the lattice residuals.
+
+    `solve(pa_points, f_points)` returns the solver's outputs [n, 2] (log10
+    collapse strength, max R/R_E).  A lattice cell is integrated in full when
+    its corner strengths spread by more than `cell_spread` (relative), or when
+    the corrected network strength differs from the bilinear interpolation of
+    the corner solutions by more than `cell_disagreement` (relative) anywhere
+    inside it; a random `audit_fraction` of the other points is integrated too
+    and measures the error of what is served."""
+    t0 = time.perf_counter()
+    n_pa, n_f = len(pa), len(f_khz)
+    PA, FR = np.meshgrid(pa, f_khz, indexing="ij")
+    ia, ca, ta = _lattice_axis(n_pa, stride)
+    ib, cb, tb = _lattice_axis(n_f, stride)
+    lat = np.zeros((n_pa, n_f), bool)
+    lat[np.ix_(ia, ib)] = True
+    solve_s = 0.0
+    t1 = time.perf_counter()
+    sol = np.zeros((n_pa, n_f, 2))
+    sol[lat] = solve(PA[lat], FR[lat])
+    solve_s += time.perf_counter() - t1
+    pred = mlp.predict(features(PA.ravel(), FR.ravel(), radii_um)).reshape(n_pa, n_f, 2).astype(np.float64)
+    res = np.where(lat[..., None], sol - pred, 0.0)
+    # bilinear interpolation inside each cell: corners (a, b), (a+1, b), (a, b+1), (a+1, b+1)
+    A0, A1 = ia[ca][:, None], ia[ca + 1][:, None]
+    B0, B1 = ib[cb][None, :], ib[cb + 1][None, :]
+    wa, wb = ta[:, None, None], tb[None, :, None]
+
+    def bil(v):
+        return ((1 - wa) * (1 - wb) * v[A0, B0] + wa * (1 - wb) * v[A1, B0] + (1 - wa) * wb * v[A0, B1]
+                + wa * wb * v[A1, B1])
+
+    corr = pred + bil(res)
+    interp = bil(sol)
+    # per cell: corner spread of the strength and the largest corrected-vs-interpolated departure
+    nca, ncb = len(ia) - 1, len(ib) - 1
+    cs = sol[..., 0]
+    corners = np.stack([cs[np.ix_(ia[:-1], ib[:-1])], cs[np.ix_(ia[1:], ib[:-1])], cs[np.ix_(ia[:-1], ib[1:])],
+                        cs[np.ix_(ia[1:], ib[1:])]])
+    spread = 10.0 ** (corners.max(0) - corners.min(0)) - 1.0
+    dep = np.abs(10.0 ** (corr[..., 0] - interp[..., 0]) - 1.0)
+    dep_cell = np.zeros((nca, ncb))
+    np.maximum.at(dep_cell, (np.broadcast_to(ca[:, None], dep.shape), np.broadcast_to(cb[None, :], dep.shape)), dep)
+    bad = (spread > cell_spread) | (dep_cell > cell_disagreement)
+    flag = np.zeros((n_pa, n_f), bool)
+    for a, b in np.argwhere(bad):
+        flag[ia[a]:ia[a + 1] + 1, ib[b]:ib[b + 1] + 1] = True
+    rng = np.random.default_rng(seed)
+    audit = (rng.random((n_pa, n_f)) < audit_fraction) & ~flag & ~lat
+    todo = (flag | audit) & ~lat
+    t1 = time.perf_counter()
+    if todo.any():
+        sol[todo] = solve(PA[todo], FR[todo])
+    solve_s += time.perf_counter() - t1
+    integrated = lat | todo
+    out = np.where(integrated[..., None], sol, corr)
+    err = 0.0
+    if audit.any():
+        s_true = 10.0 ** sol[audit][:, 0]
+        err = float(np.max(np.abs(10.0 ** corr[audit][:, 0] - s_true) / s_true))
+    return LatticeScreenResult(map=out, integrated=integrated, lattice=lat, audited=audit,
+                               audit_max_rel_error=err, solve_seconds=solve_s, seconds=time.perf_counter() - t0)
