@@ -41,7 +41,7 @@ namespace {
 enum BufId {
     B_TIME_DOMAIN, B_ACTUAL_TIME, B_STATE, B_UPAR, B_SPAR, B_GPAR, B_IGPAR, B_UACC, B_IUACC, B_SACC, B_ISACC,
     B_COUPLING, B_COUPLING_STRENGTH, B_COUPLING_INDEX, B_DENSE_INDEX, B_DENSE_TIME, B_DENSE_STATE,
-    B_RTOL, B_ATOL, B_CNT_ACC, B_CNT_REJ, B_CNT_BICG, B_CNT_RHS, B_STATUS, B_COUNT
+    B_RTOL, B_ATOL, B_CROW, B_CCOL, B_CNT_ACC, B_CNT_REJ, B_CNT_BICG, B_CNT_RHS, B_STATUS, B_COUNT
 };
 
 struct Buf {
@@ -90,6 +90,7 @@ struct bes_solver {
     long long max_steps = 1000000;
     /* launch plan */
     bool order_dirty = true;
+    bool scaled_coupling[2] = {false, false};   /* a host copy of CouplingRow/ColumnScale with a value != 1 went to the device */
     int class_begin[3] = {0, 0, 0}, class_count[3] = {0, 0, 0};
     bool class0_all32 = false;
     bool class_shared[3] = {false, false, false};   /* every system of the class uses one matrix */
@@ -154,6 +155,8 @@ int var_to_buf(int var) {
         case BES_DENSE_STATE: return B_DENSE_STATE;
         case BES_RELATIVE_TOLERANCE_SYSTEM: return B_RTOL;
         case BES_ABSOLUTE_TOLERANCE_SYSTEM: return B_ATOL;
+        case BES_COUPLING_ROW_SCALE: return B_CROW;
+        case BES_COUPLING_COLUMN_SCALE: return B_CCOL;
         default: return -1;
     }
 }
@@ -182,6 +185,8 @@ const char* var_name(int var) {
         case BES_RELATIVE_TOLERANCE_SYSTEM: return "RelativeToleranceSystem";
         case BES_ABSOLUTE_TOLERANCE_SYSTEM: return "AbsoluteToleranceSystem";
         case BES_COUNTERS: return "Counters";
+        case BES_COUPLING_ROW_SCALE: return "CouplingRowScale";
+        case BES_COUPLING_COLUMN_SCALE: return "CouplingColumnScale";
         default: return "unknown";
     }
 }
@@ -199,6 +204,12 @@ int units_class(int n) { return n <= 32 ? 0 : (n <= 64 ? 1 : 2); }
 bes_status copy_h2d(bes_solver* h, int id) {
     Buf& b = h->buf[id];
     if (b.count > 0) CUDA_TRY(h, cudaMemcpyAsync(b.d, b.h, b.bytes(), cudaMemcpyHostToDevice, h->stream));
+    if (id == B_CROW || id == B_CCOL) {
+        const double* v = (const double*)b.h;
+        bool any = false;
+        for (int64_t i = 0; i < b.count && !any; i++) any = v[i] != 1.0;
+        h->scaled_coupling[id == B_CCOL] = any;
+    }
     return BES_OK;
 }
 bes_status copy_d2h(bes_solver* h, int id) {
@@ -287,6 +298,8 @@ DeviceProblem make_problem(bes_solver* h) {
     P.time_domain = (double*)h->buf[B_TIME_DOMAIN].d;
     P.actual_time = (double*)h->buf[B_ACTUAL_TIME].d;
     P.rtol = (const double*)h->buf[B_RTOL].d;
+    P.coupling_row_scale = (const double*)h->buf[B_CROW].d;
+    P.coupling_col_scale = (const double*)h->buf[B_CCOL].d;
     P.atol = (const double*)h->buf[B_ATOL].d;
     P.event_tol = h->d_event_tol;
     P.event_dir = h->d_event_dir;
@@ -531,7 +544,7 @@ bes_status bes_create(const bes_config* c, bes_solver** out) {
         {B_IUACC, h->niua * TU}, {B_SACC, h->nsa * NS}, {B_ISACC, h->nisa * NS}, {B_COUPLING, moff},
         {B_COUPLING_STRENGTH, h->nc * NS}, {B_COUPLING_INDEX, h->nc}, {B_DENSE_INDEX, NS},
         {B_DENSE_TIME, h->ndo * NS}, {B_DENSE_STATE, (int64_t)h->ndo * h->ud * TU}, {B_RTOL, h->ud * NS},
-        {B_ATOL, h->ud * NS}, {B_CNT_ACC, NS}, {B_CNT_REJ, NS}, {B_CNT_BICG, NS}, {B_CNT_RHS, NS}, {B_STATUS, NS}};
+        {B_ATOL, h->ud * NS}, {B_CROW, TU}, {B_CCOL, TU}, {B_CNT_ACC, NS}, {B_CNT_REJ, NS}, {B_CNT_BICG, NS}, {B_CNT_RHS, NS}, {B_STATUS, NS}};
     size_t total_bytes = 0;
     for (auto& sz : sizes) {
         Buf& b = h->buf[sz.id];
@@ -593,6 +606,12 @@ bes_status bes_create(const bes_config* c, bes_solver** out) {
     for (int64_t i = 0; i < h->ud * NS; i++) { rt[i] = 1e-8; at[i] = 1e-8; }
     CREATE_TRY(cudaMemcpy(h->buf[B_RTOL].d, rt, h->buf[B_RTOL].bytes(), cudaMemcpyHostToDevice));
     CREATE_TRY(cudaMemcpy(h->buf[B_ATOL].d, at, h->buf[B_ATOL].bytes(), cudaMemcpyHostToDevice));
+    /* coupling factors a_i = b_j = 1: every system's matrix is the stored one */
+    for (int id : {B_CROW, B_CCOL}) {
+        double* v = (double*)h->buf[id].h;
+        for (int64_t i = 0; i < TU; i++) v[i] = 1.0;
+        CREATE_TRY(cudaMemcpy(h->buf[id].d, v, h->buf[id].bytes(), cudaMemcpyHostToDevice));
+    }
     h->event_tol.assign(std::max(1, h->ne), 1e-6);
     h->event_dir.assign(std::max(1, h->ne), 0);
     CREATE_TRY(cudaMemcpy(h->d_event_tol, h->event_tol.data(), sizeof(double) * h->event_tol.size(), cudaMemcpyHostToDevice));
@@ -713,6 +732,8 @@ static bes_status unit_slot(bes_solver* h, const char* fn, int sid, int uid, int
         case BES_UNIT_PARAMETERS: id = B_UPAR; lim = h->nup; break;
         case BES_UNIT_ACCESSORIES: id = B_UACC; lim = h->nua; break;
         case BES_INTEGER_UNIT_ACCESSORIES: id = B_IUACC; lim = h->niua; break;
+        case BES_COUPLING_ROW_SCALE: id = B_CROW; lim = 1; break;
+        case BES_COUPLING_COLUMN_SCALE: id = B_CCOL; lim = 1; break;
         default: return fail(h, BES_ERR_OPTION, "%s: variable %s needs a different argument list", fn, var_name(var));
     }
     if ((st = bound(h, fn, var_name(var), k, 0, lim - 1))) return st;
@@ -922,7 +943,7 @@ static bes_status transfer(bes_solver* h, int32_t var, bool to_device) {
         case BES_ALL: {
             const int ids[] = {B_TIME_DOMAIN, B_ACTUAL_TIME, B_STATE, B_UPAR, B_SPAR, B_GPAR, B_IGPAR, B_UACC,
                                B_IUACC, B_SACC, B_ISACC, B_COUPLING, B_COUPLING_STRENGTH, B_COUPLING_INDEX,
-                               B_DENSE_INDEX, B_DENSE_TIME, B_DENSE_STATE, B_RTOL, B_ATOL};
+                               B_DENSE_INDEX, B_DENSE_TIME, B_DENSE_STATE, B_RTOL, B_ATOL, B_CROW, B_CCOL};
             for (int id : ids)
                 if ((st = one(id))) return st;
             if (!to_device) {
@@ -982,6 +1003,13 @@ bes_status bes_solve_periods(bes_solver* h, int32_t n_periods, int32_t reset_at)
     ClassLaunch L[3] = {};
     for (int cls = 0; cls < 3; cls++)
         if (h->class_count[cls] > 0 && (st = plan_class(h, cls, &L[cls]))) return st;
+    if (h->scaled_coupling[0] || h->scaled_coupling[1])
+        for (int cls = 0; cls < 3; cls++)
+            if (h->class_count[cls] > 0 && L[cls].v.rhs != 3)
+                return fail(h, BES_ERR_ARGUMENT,
+                            "bes_solve_periods: CouplingRowScale / CouplingColumnScale hold values other than 1, "
+                            "which only the shared-matrix kernels apply: turn SharedCouplingMatrices on and give "
+                            "every system of a size class the same matrix (systems of more than 32 units)");
     if (!h->use_graph) {
         CUDA_TRY(h, cudaEventRecord(h->t0, h->stream));
         if ((st = enqueue_solve(h, P, h->stream, L, &h->last_launches))) return st;

@@ -7,7 +7,9 @@
  *   system scope component k of system s at [k*n_systems + s]
  *                (time domain, actual time, tolerances, system parameters/accessories);
  *   coupling     one N x N column-major matrix per distinct geometry, system s uses the
- *                matrix at coupling_offset[s] (systems may share one matrix).
+ *                matrix at coupling_offset[s] (systems may share one matrix); with the
+ *                shared-matrix kernels the matrix of unit pair (i, j) is a_i G_ij b_j,
+ *                a and b unit-scope factors (1 unless set).
  * This is the reference's layout (SourceCodes/CoupledSystems_PerBlock_Interface.cuh:875-879,
  * :918-919, :1007, :1124-1125) with the per-block thread padding removed and ragged
  * unit counts allowed.
@@ -27,6 +29,8 @@ struct DeviceProblem {
     const int64_t* unit_offset;      /* [n_systems] */
     const int64_t* coupling_offset;  /* [n_systems] offset (doubles) of the system's matrix */
     const double* coupling;
+    const double* coupling_row_scale;  /* [total_units] a_i, or NULL: the shared-matrix kernels use  */
+    const double* coupling_col_scale;  /* [total_units] b_j    C_ij = a_i G_ij b_j with G the stored matrix */
     const int32_t* order;            /* [n_active] processing order (costliest first) */
     double* state;                   /* [UD][total_units] */
     const double* upar;              /* [NUP][total_units] */

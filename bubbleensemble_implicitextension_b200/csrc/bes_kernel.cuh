@@ -601,21 +601,26 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
 
 /* ---------------------------------------------------------------------------
  * Coupled right-hand side with the launch's shared coupling matrix staged once
- * per CTA (RHS = 3, 64 or 128 units).  The products apply C to scaled vectors,
- *   A x0 = rD (C (X1sq x0)),  A p = p + rD (C (X1sq p)),
- *   A^T p~ = p~ + X1sq (C^T (rD p~)),
- * with C row sums as four interleaved fma chains and C column sums in the
+ * per CTA (RHS = 3, 64 or 128 units).  A system's coupling matrix is
+ * C = diag(a) G diag(b) with G the staged matrix and a, b unit-scope factors
+ * (1 unless the caller sets them: one shared geometry, per-system radii).
+ * With u = b X1sq and v = rD a the products apply G to scaled vectors,
+ *   A x0 = v (G (u x0)),  A p = p + v (G (u p)),  A^T p~ = p~ + u (G^T (v p~)),
+ *   right-hand side v (G (b CPT)) + x_u,
+ * with G row sums as four interleaved fma chains and G column sums in the
  * halving-tree order over 32UG; the oracle's shared-matrix association
- * computes the same. */
+ * computes the same (a = b = 1 reproduces the unscaled products bit for bit). */
 template <int U, int G>
 __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const DeviceProblem& P, double T,
                                                    double (&Xs)[U][UD], double (&F)[U][UD],
                                                    double (&up)[U][NUPa], double (&ua)[U][NUAa],
-                                                   int (&iua)[U][NIUAa], bool& capped) {
+                                                   int (&iua)[U][NIUAa], const double (&ra)[U],
+                                                   const double (&cb)[U], bool& capped) {
     constexpr int NMAX = SharedCSmem<U, G>::NMAX;
     constexpr int LDC = SharedCSmem<U, G>::LDC;
     constexpr int H = NMAX / 2;
     const int N = S.N;
+    /* with C = diag(a) G diag(b): x1 holds u = b X1sq (applied before G), rd holds v = rD a (after G) */
     double xu[U], rd[U], x1[U], r[U], rt[U], x[U], p[U], pt[U];
     grp_sync(S);
 #pragma unroll
@@ -628,10 +633,10 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const Dev
 #pragma unroll
             for (int k = 0; k < UD; k++) F[m][k] = Fl[k];
             xu[m] = Fl[IC];
-            rd[m] = cpf;
-            x1[m] = Xs[m][0] * Xs[m][0];
-            S.vcpt[i] = cpt;
-            S.vp[i] = x1[m] * xu[m];   /* z0 = X1sq x0 */
+            rd[m] = cpf * ra[m];
+            x1[m] = cb[m] * (Xs[m][0] * Xs[m][0]);
+            S.vcpt[i] = cb[m] * cpt;
+            S.vp[i] = x1[m] * xu[m];   /* z0 = b X1sq x0 */
         } else {
 #pragma unroll
             for (int k = 0; k < UD; k++) F[m][k] = 0.0;
@@ -776,11 +781,12 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const Dev
 template <int U, int RHS, int G>
 __device__ __forceinline__ int rhs_eval(const Sys<U, G>& S, const DeviceProblem& P, double T, double (&Xs)[U][UD],
                                         double (&F)[U][UD], double (&up)[U][NUPa], double (&ua)[U][NUAa],
-                                        int (&iua)[U][NIUAa], bool& capped) {
+                                        int (&iua)[U][NIUAa], const double (&ra)[U], const double (&cb)[U],
+                                        bool& capped) {
     if constexpr (RHS == 0) {
         return coupled_rhs<U, G>(S, P, T, Xs, F, up, ua, iua, capped);
     } else if constexpr (RHS == 3) {
-        return coupled_rhs_sharedc<U, G>(S, P, T, Xs, F, up, ua, iua, capped);
+        return coupled_rhs_sharedc<U, G>(S, P, T, Xs, F, up, ua, iua, ra, cb, capped);
     } else {
         static_assert(U == 1, "the register-resident operator needs one unit per lane");
         return coupled_rhs_regw<RHS == 2 ? 32 : 0>(S, P, T, Xs, F, up, ua, iua, capped);
@@ -795,6 +801,7 @@ struct Lane {
     double ua[U][NUAa];
     int iua[U][NIUAa];
     double ev_a[U][NEa], ev_n[U][NEa];
+    double ra[U], cb[U];   /* coupling factors a_i, b_i of the shared-matrix kernels */
 };
 
 struct Counters {
@@ -864,7 +871,7 @@ __device__ __forceinline__ bool step_rkck45(const Sys<U, G>& S, const DeviceProb
                     Xs[m][c] = fma(acc, dt, L.X[m][c]);
                 }
         }
-        cnt.bicg += rhs_eval<U, RHS, G>(S, P, Ts, Xs, F, L.up, L.ua, L.iua, capped);
+        cnt.bicg += rhs_eval<U, RHS, G>(S, P, Ts, Xs, F, L.up, L.ua, L.iua, L.ra, L.cb, capped);
 #pragma unroll
         for (int j = 0; j < 6; j++)
 #pragma unroll
@@ -931,7 +938,7 @@ __device__ __forceinline__ bool step_rk4(const Sys<U, G>& S, const DeviceProblem
                     Xs[m][c] = st == 3 ? fma(kprev, dt, L.X[m][c]) : fma(kprev * kRK4_A[st], dt, L.X[m][c]);
                 }
         }
-        cnt.bicg += rhs_eval<U, RHS, G>(S, P, Ts, Xs, F, L.up, L.ua, L.iua, capped);
+        cnt.bicg += rhs_eval<U, RHS, G>(S, P, Ts, Xs, F, L.up, L.ua, L.iua, L.ra, L.cb, capped);
 #pragma unroll
         for (int j = 0; j < 4; j++)
 #pragma unroll
@@ -1332,6 +1339,13 @@ __global__ void __launch_bounds__(RHS == 3 || G > 1 ? 256 : 128, 1) bes_ensemble
             } else {
 #pragma unroll
                 for (int c = 0; c < NUP; c++) L.up[m][c] = v ? __ldg(P.upar + (int64_t)c * S.tot + g) : 0.0;
+            }
+            if constexpr (RHS == 3) {
+                L.ra[m] = v ? (P.coupling_row_scale ? __ldg(P.coupling_row_scale + g) : 1.0) : 0.0;
+                L.cb[m] = v ? (P.coupling_col_scale ? __ldg(P.coupling_col_scale + g) : 1.0) : 0.0;
+            } else {
+                L.ra[m] = 1.0;
+                L.cb[m] = 1.0;
             }
             for (int c = 0; c < NUA; c++) L.ua[m][c] = v ? P.uacc[(int64_t)c * S.tot + g] : 0.0;
 #pragma unroll

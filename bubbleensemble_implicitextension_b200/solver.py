@@ -47,6 +47,8 @@ class ListOfVariables(IntEnum):
     RelativeToleranceSystem = 100
     AbsoluteToleranceSystem = 101
     Counters = 102
+    CouplingRowScale = 103
+    CouplingColumnScale = 104
 
 
 class ListOfSolverOptions(IntEnum):

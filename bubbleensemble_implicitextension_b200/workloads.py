@@ -139,6 +139,8 @@ class Ensemble:
     reset_at: int = 32
     max_steps_per_period: int = 1_000_000
     shared_matrices: bool = False     # SharedCouplingMatrices: stage the launch's one matrix per CTA
+    coupling_row_scale: Optional[np.ndarray] = None   # [TU] a_i of C_ij = a_i G_ij b_j (shared geometry G)
+    coupling_col_scale: Optional[np.ndarray] = None   # [TU] b_j
     name: str = ""
     info: dict = dataclasses.field(default_factory=dict)
 
@@ -189,7 +191,9 @@ class Ensemble:
         return dataclasses.replace(
             self, units=self.units[systems].copy(), upar=self.upar[:, cols].copy(), state=self.state[:, cols].copy(),
             coupling=np.concatenate(blocks), matrix_of_system=np.asarray(new_mos, dtype=np.int32),
-            rtol=self.rtol[:, systems].copy(), atol=self.atol[:, systems].copy(), info=dict(self.info))
+            rtol=self.rtol[:, systems].copy(), atol=self.atol[:, systems].copy(), info=dict(self.info),
+            coupling_row_scale=None if self.coupling_row_scale is None else self.coupling_row_scale[cols].copy(),
+            coupling_col_scale=None if self.coupling_col_scale is None else self.coupling_col_scale[cols].copy())
 
     def make_solver(self, device: int = 0, **kw) -> S.ProblemSolver:
         """Create a ProblemSolver filled with this ensemble (host mirrors only; call H2D)."""
@@ -225,6 +229,10 @@ class Ensemble:
         ps.set_accessory_reset(np.zeros(NUA), np.array([-1], dtype=np.int32))
         if self.shared_matrices:
             ps.SolverOption(O.SharedCouplingMatrices, 1)
+        if self.coupling_row_scale is not None:
+            ps.set_array(V.CouplingRowScale, self.coupling_row_scale)
+        if self.coupling_col_scale is not None:
+            ps.set_array(V.CouplingColumnScale, self.coupling_col_scale)
 
 
 def c1_ensemble(n_pa: int = 16, n_f: int = 16, n_units: int = 32, spacing_um: float = 150.0,
@@ -331,6 +339,54 @@ def c3_ensemble(n_systems: int = 4096, n_units: int = 128, seed: int = 3, n_peri
                     coupling=C.T.reshape(-1).copy(), matrix_of_system=np.zeros(n_systems, dtype=np.int32),
                     rtol=np.full((2, n_systems), rtol), atol=np.full((2, n_systems), rtol), n_periods=n_periods,
                     reset_at=reset_at, shared_matrices=True, name=f"c3_{n_systems}x{n_units}_shared")
+
+
+def c3_radii_ensemble(n_systems: int = 4096, n_units: int = 128, seed: int = 3, n_periods: int = 4,
+                      reset_at: int = -1, cube_um: float = 1000.0, pa_bar: float = 1.2, f_khz: float = 200.0,
+                      rtol: float = 1e-10) -> Ensemble:
+    """Shared geometry, per-system radii: one N-bubble cloud (uniform in a cube,
+    PCG64(seed)) whose geometric matrix G_ij = 1/d_ij every system shares, and
+    for system s its own equilibrium radii (lognormal median 4 um, sigma 0.4,
+    clipped to [1, 12] um, PCG64(seed + s)).  System s couples through
+    C_ij = R_i^-2 G_ij R_j^3 -- the reference-format matrix of its radii --
+    given to the library as the shared G with the unit factors
+    a_i = R_i^-2, b_j = R_j^3.  All systems start from rest."""
+    rng = np.random.default_rng(seed)
+    pts = rng.uniform(0.0, cube_um, (n_units, 3))
+    d = np.sqrt(((pts[:, None, :] - pts[None, :, :]) ** 2).sum(-1))
+    off = ~np.eye(n_units, dtype=bool)
+    G = np.zeros((n_units, n_units))
+    G[off] = 1.0 / d[off]
+    radii = np.stack([np.clip(np.exp(np.log(4.0) + 0.4 * np.random.default_rng(seed + s).standard_normal(n_units)),
+                              1.0, 12.0) for s in range(n_systems)])
+    upar = km_unit_parameters(pa_bar, f_khz, 0.0, 0.0, 0.0, radii).reshape(NUP, -1)
+    state = np.zeros((2, n_systems * n_units))
+    state[0] = 1.0
+    r = radii.reshape(-1)
+    return Ensemble(units=np.full(n_systems, n_units, dtype=np.int32), upar=upar, state=state,
+                    coupling=G.T.reshape(-1).copy(), matrix_of_system=np.zeros(n_systems, dtype=np.int32),
+                    rtol=np.full((2, n_systems), rtol), atol=np.full((2, n_systems), rtol), n_periods=n_periods,
+                    reset_at=reset_at, shared_matrices=True, coupling_row_scale=1.0 / (r * r),
+                    coupling_col_scale=r * r * r, name=f"c3_radii_{n_systems}x{n_units}")
+
+
+def explicit_matrices(ens: Ensemble) -> Ensemble:
+    """The same ensemble with each system's factored matrix a_i G_ij b_j written
+    out as its own matrix (no factors, no shared staging)."""
+    if ens.coupling_row_scale is None and ens.coupling_col_scale is None:
+        return ens
+    moff = ens.matrix_offsets()
+    uoff = ens.unit_offset
+    blocks = []
+    for s in range(ens.n_systems):
+        n = int(ens.units[s])
+        G = ens.coupling[moff[ens.matrix_of_system[s]]:][:n * n].reshape(n, n).T    # row-major view of column-major
+        a = np.ones(n) if ens.coupling_row_scale is None else ens.coupling_row_scale[uoff[s]:uoff[s] + n]
+        b = np.ones(n) if ens.coupling_col_scale is None else ens.coupling_col_scale[uoff[s]:uoff[s] + n]
+        blocks.append((a[:, None] * G * b[None, :]).T.reshape(-1))
+    return dataclasses.replace(ens, coupling=np.concatenate(blocks),
+                               matrix_of_system=np.arange(ens.n_systems, dtype=np.int32), shared_matrices=False,
+                               coupling_row_scale=None, coupling_col_scale=None)
 
 
 def collapse_records(uacc: np.ndarray, iuacc: np.ndarray, units: np.ndarray):

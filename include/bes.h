@@ -67,6 +67,13 @@ typedef int32_t bes_status;
 #define BES_RELATIVE_TOLERANCE_SYSTEM 100  /* [UD][n_systems] per-system relative tolerances */
 #define BES_ABSOLUTE_TOLERANCE_SYSTEM 101  /* [UD][n_systems] per-system absolute tolerances */
 #define BES_COUNTERS 102                   /* per-system counters and status (device -> host only) */
+#define BES_COUPLING_ROW_SCALE 103         /* [total_units] a_i and                                        */
+#define BES_COUPLING_COLUMN_SCALE 104      /* [total_units] b_j of a system's coupling matrix
+                                              C_ij = a_i G_ij b_j, G the stored (shared) matrix; default 1.
+                                              One geometry G = 1/d_ij serves systems with their own radii
+                                              (a_i = R_i^-2, b_j = R_j^3).  Applied by the shared-matrix
+                                              kernels only (SharedCouplingMatrices, more than 32 units);
+                                              a solve with other launches and factors != 1 is an error. */
 
 /* ListOfSolverOptions, same names and order as Interface.cuh:55-68 */
 #define BES_OPT_INITIAL_TIME_STEP 0

@@ -117,12 +117,12 @@ inline double tree_max(const double* v, int n, double* tmp) {
 
 struct Work {
     int N;
-    std::vector<double> cpt, rd, x1sq, xu, b, r, rt, p, pt, q, qt, x, W, tmp, tmp2;
+    std::vector<double> cpt, rd, x1sq, xu, b, r, rt, p, pt, q, qt, x, W, tmp, tmp2, us, vs;
     explicit Work(int n) : N(n) {
         int P = next_pow2_32(n);
         cpt.resize(n); rd.resize(n); x1sq.resize(n); xu.resize(n); b.resize(n);
         r.resize(n); rt.resize(n); p.resize(n); pt.resize(n); q.resize(n); qt.resize(n);
-        x.resize(n); W.resize((size_t)n * n); tmp.resize(P); tmp2.resize(n);
+        x.resize(n); W.resize((size_t)n * n); tmp.resize(P); tmp2.resize(n); us.resize(n); vs.resize(n);
     }
 };
 
@@ -134,7 +134,8 @@ struct Work {
  * iteration limit was used up without meeting an exit test. */
 int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
                 const double* up, long ups, const double* C, int max_iter,
-                double* f0, double* f1, bool* capped, bool shared_assoc = false) {
+                double* f0, double* f1, bool* capped, bool shared_assoc = false,
+                const double* ra = nullptr, const double* cb = nullptr) {
     const int N = w.N;
     double upl[NUP];
     for (int i = 0; i < N; i++) {
@@ -142,14 +143,28 @@ int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
         km_ode(y0[i], y1[i], T, upl, &f0[i], &w.xu[i], &w.cpt[i], &w.rd[i]);
         w.x1sq[i] = y0[i] * y0[i];
     }
+    if (shared_assoc) {
+        /* C = diag(a) G diag(b): u = b X1sq before G, v = rD a after G (a = b = 1 without factors) */
+        for (int i = 0; i < N; i++) {
+            w.us[i] = (cb ? cb[i] : 1.0) * w.x1sq[i];
+            w.vs[i] = w.rd[i] * (ra ? ra[i] : 1.0);
+            w.tmp2[i] = (cb ? cb[i] : 1.0) * w.cpt[i];
+        }
+    }
     /* b = rD (C CPT) + x_u ; r = b - A x_u  (Steppers.cuh:495-505, :576-584, :647-666) */
     for (int i = 0; i < N; i++) {
-        double bi = row_sum4(N, [&](int j) { return C[i + (long)j * N]; }, [&](int j) { return w.cpt[j]; });
-        bi = fma(w.rd[i], bi, w.xu[i]);
-        double ax = shared_assoc
-                        ? row_sum4(N, [&](int j) { return C[i + (long)j * N]; }, [&](int j) { return w.x1sq[j] * w.xu[j]; })
-                        : row_sum4(N, [&](int j) { return C[i + (long)j * N] * w.x1sq[j]; }, [&](int j) { return w.xu[j]; });
-        ax = fma(w.rd[i], ax, w.xu[i]);
+        double bi, ax;
+        if (shared_assoc) {
+            bi = row_sum4(N, [&](int j) { return C[i + (long)j * N]; }, [&](int j) { return w.tmp2[j]; });
+            bi = fma(w.vs[i], bi, w.xu[i]);
+            ax = row_sum4(N, [&](int j) { return C[i + (long)j * N]; }, [&](int j) { return w.us[j] * w.xu[j]; });
+            ax = fma(w.vs[i], ax, w.xu[i]);
+        } else {
+            bi = row_sum4(N, [&](int j) { return C[i + (long)j * N]; }, [&](int j) { return w.cpt[j]; });
+            bi = fma(w.rd[i], bi, w.xu[i]);
+            ax = row_sum4(N, [&](int j) { return C[i + (long)j * N] * w.x1sq[j]; }, [&](int j) { return w.xu[j]; });
+            ax = fma(w.rd[i], ax, w.xu[i]);
+        }
         w.r[i] = bi - ax;
         w.rt[i] = w.r[i];
         w.x[i] = w.xu[i];
@@ -173,15 +188,15 @@ int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
         }
         /* q = A p (row sums) and qt = A^T pt (tree sums), Steppers.cuh:669-706 */
         if (shared_assoc) {
-            for (int j = 0; j < N; j++) { w.b[j] = w.x1sq[j] * w.p[j]; w.xu[j] = w.rd[j] * w.pt[j]; }
-            /* w.b, w.xu reused as the scaled vectors z = X1sq p and z~ = rD p~ (x_u is no longer needed) */
+            for (int j = 0; j < N; j++) { w.b[j] = w.us[j] * w.p[j]; w.xu[j] = w.vs[j] * w.pt[j]; }
+            /* w.b, w.xu reused as the scaled vectors z = u p and z~ = v p~ (x_u is no longer needed) */
         }
         for (int i = 0; i < N; i++) {
             if (shared_assoc) {
                 double s = row_sum4(N, [&](int j) { return C[i + (long)j * N]; }, [&](int j) { return w.b[j]; });
-                w.q[i] = fma(w.rd[i], s, w.p[i]);
+                w.q[i] = fma(w.vs[i], s, w.p[i]);
                 for (int j = 0; j < N; j++) w.tmp2[j] = C[j + (long)i * N] * w.xu[j];
-                w.qt[i] = fma(w.x1sq[i], tree_sum(w.tmp2.data(), N, w.tmp.data()), w.pt[i]);
+                w.qt[i] = fma(w.us[i], tree_sum(w.tmp2.data(), N, w.tmp.data()), w.pt[i]);
             } else {
                 w.q[i] = w.p[i] + row_sum4(N, [&](int j) { return w.W[i + (long)j * N]; }, [&](int j) { return w.p[j]; });
                 for (int j = 0; j < N; j++) w.tmp2[j] = w.W[j + (long)i * N] * w.pt[j];
@@ -244,7 +259,9 @@ struct SystemRun {
     int rhs(double T, const double* a0, const double* a1, double* f0, double* f1, int64_t& nbicg, bool& capped_any) {
         bool capped = false;
         int it = coupled_rhs(w, T, a0, a1, up(), tot, C(), P->bicg_max_iter, f0, f1, &capped,
-                             P->shared_assoc != 0 && N > 32);
+                             P->shared_assoc != 0 && N > 32,
+                             P->coupling_row_scale ? P->coupling_row_scale + off : nullptr,
+                             P->coupling_col_scale ? P->coupling_col_scale + off : nullptr);
         nbicg += it;
         if (capped) capped_any = true;
         return it;

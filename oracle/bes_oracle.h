@@ -79,6 +79,10 @@ typedef struct bes_oracle_problem {
     int64_t* n_bicg_iter;
     int64_t* n_rhs;
     int32_t* status;
+    /* coupling factors of the shared-matrix association, [total_units] each, or NULL (= 1):
+     * system s couples units i, j through a_i G_ij b_j, G its stored matrix */
+    const double* coupling_row_scale;
+    const double* coupling_col_scale;
 } bes_oracle_problem;
 
 /* Integrate `n_periods` reference Solve() calls for every active system.

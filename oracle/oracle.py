@@ -35,7 +35,7 @@ class Problem(ctypes.Structure):
         ("ndo", ctypes.c_int32), ("do_save_frequency", ctypes.c_int32), ("do_min_dt", ctypes.c_double),
         ("dense_time", _dp), ("dense_state", _dp), ("dense_index", _i32p),
         ("n_accepted", _i64p), ("n_rejected", _i64p), ("n_bicg_iter", _i64p), ("n_rhs", _i64p),
-        ("status", _i32p),
+        ("status", _i32p), ("coupling_row_scale", _dp), ("coupling_col_scale", _dp),
     ]
 
 
@@ -130,6 +130,12 @@ def run(ens, n_periods: int = None, reset_at: int = None, threads: int = 0, syst
     # the library stages a launch's one shared matrix per CTA (and associates the products
     # accordingly) when the ensemble asks for shared coupling matrices
     P.shared_assoc = int(getattr(ens, "shared_matrices", False) if shared_assoc is None else shared_assoc)
+    # per-unit coupling factors (a_i G_ij b_j) of a shared geometry, if the ensemble has them
+    for k, attr in (("coupling_row_scale", "coupling_row_scale"), ("coupling_col_scale", "coupling_col_scale")):
+        v = getattr(ens, attr, None)
+        if v is not None:
+            a[k] = np.ascontiguousarray(v, np.float64)
+            setattr(P, k, _p(a[k], _dp))
     P.max_steps_per_period = ens.max_steps_per_period
     P.ndo = ndo
     P.do_save_frequency = do_save_frequency

@@ -125,3 +125,27 @@ def test_multi_warp_groups_pull_many_systems(gpu):
     c = run_gpu(ens, n_periods=1, reset_at=-1, warps_per_block=2)
     assert_bitwise(b, a, KEYS)
     assert_bitwise(c, a, KEYS)
+
+
+@pytest.mark.parametrize("n,wps", [(128, 0), (100, 1), (64, 0)])
+def test_shared_geometry_with_per_system_radii(n, wps, gpu, oracle_lib):
+    """One staged geometry G for the launch, each system's own radii through the
+    unit factors a_i = R_i^-2, b_j = R_j^3 (C_ij = a_i G_ij b_j)."""
+    ens = bounded(W.c3_radii_ensemble(n_systems=5, n_units=n, seed=40 + n, n_periods=1,
+                                      cube_um=400.0 * (n / 32) ** (1 / 3)))
+    got = run_gpu(ens, n_periods=1, reset_at=-1, warps_per_block=8, warps_per_system=wps)
+    want = oracle_lib.run(ens, n_periods=1, reset_at=-1)
+    assert_bitwise(got, want, KEYS)
+
+
+def test_coupling_factors_need_the_shared_matrix_kernels(gpu):
+    """Factors other than 1 on a launch without the shared-matrix kernels are refused."""
+    ens = W.c3_radii_ensemble(n_systems=2, n_units=40, n_periods=1)
+    ens.shared_matrices = False
+    ps = ens.make_solver()
+    try:
+        ps.SynchroniseFromHostToDevice(S.ListOfVariables.All)
+        with pytest.raises(S.BesError, match="CouplingRowScale"):
+            ps.solve_periods(1, -1)
+    finally:
+        ps.close()
