@@ -101,6 +101,8 @@ def parse():
     ap.add_argument("--sweep-spread", type=float, default=0.05)
     ap.add_argument("--sweep-disagreement", type=float, default=0.02)
     ap.add_argument("--sweep-dump", type=str, default="", help="c5_sweep: write the maps to this .npz")
+    ap.add_argument("--autotune", type=int, default=1, choices=[0, 1],
+                    help="1: pick launch shapes with bes_autotune before the warm-up (untimed)")
     ap.add_argument("--warps-per-system", type=int, default=0, choices=[0, 1],
                     help="0: systems above 32 units on 2 or 4 warps (default); 1: one warp per system")
     return ap.parse_args()
@@ -248,6 +250,7 @@ def run_b200(args, rank, world, local):
     load_inputs()
     ps.SynchroniseFromHostToDevice(V.All)
     torch.cuda.synchronize()
+    tuned = ps.autotune(n_periods=1, step_cap=2000) if args.autotune and not args.warps_per_system else None
 
     def device_step():
         # untimed: the step's inputs back in HBM (rest state), then L2 flushed
@@ -329,6 +332,7 @@ def run_b200(args, rank, world, local):
                    "total_units": ens.total_units,
                    "periods_per_step": 1,
                    "warps_per_system": "one" if args.warps_per_system else "2 or 4 above 32 units",
+                   "launch_shapes": tuned if tuned else "heuristic",
                    "l2": "flushed between timed steps (256 MiB write, untimed)",
                    "parallelism": f"{world} independent ensemble replica(s), one per GPU"},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",

@@ -104,6 +104,8 @@ struct bes_solver {
     bool graph_dirty = true;
     int use_graph = 1;
     int warps_per_system = 0;   /* 0: multi-warp systems above 32 units; 1: one warp per system */
+    int tuned_wpb[3] = {0, 0, 0};      /* per size class, set by bes_autotune (0: not tuned) */
+    int tuned_wps[3] = {-1, -1, -1};   /* per size class, set by bes_autotune (-1: not tuned) */
     float last_ms = 0.f;
     int last_launches = 0;
     std::string err;
@@ -333,13 +335,13 @@ struct ClassLaunch {
 };
 
 /* launch shape of one class (no stream work: safe before a capture) */
-bes_status plan_class(bes_solver* h, int cls, ClassLaunch* L) {
+bes_status plan_shape(bes_solver* h, int cls, int warps_per_system, int requested_wpb, ClassLaunch* L) {
     const bes::Variant v = bes::class_variant(cls, h->class0_all32, h->shared_coupling && h->class_shared[cls],
-                                         h->warps_per_system);
+                                         warps_per_system);
     const int count = h->class_count[cls];
     if (bes::max_warps_per_block(v) < v.G)
         return fail(h, BES_ERR_CUDA, "solver kernel variant (U=%d, G=%d) does not fit in shared memory", v.U, v.G);
-    const int wpb = bes::class_warps_per_block(v, count, h->sm_count, h->warps_per_block);
+    const int wpb = bes::class_warps_per_block(v, count, h->sm_count, requested_wpb);
     int per_sm = 0;
     CUDA_TRY(h, bes::occupancy(v, wpb, &per_sm));
     if (per_sm < 1)
@@ -351,6 +353,12 @@ bes_status plan_class(bes_solver* h, int cls, ClassLaunch* L) {
     L->wpb = wpb;
     L->grid = std::max(1, std::min(needed, per_sm * h->sm_count));
     return BES_OK;
+}
+
+/* the class's launch shape: the autotuner's choice if there is one, else the options */
+bes_status plan_class(bes_solver* h, int cls, ClassLaunch* L) {
+    return plan_shape(h, cls, h->tuned_wps[cls] >= 0 ? h->tuned_wps[cls] : h->warps_per_system,
+                      h->tuned_wpb[cls] > 0 ? h->tuned_wpb[cls] : h->warps_per_block, L);
 }
 
 /* the whole solve on stream s: reset the work counters, fork one stream per
@@ -665,12 +673,16 @@ bes_status bes_solver_option(bes_solver* h, int32_t option, double value) {
             if (!(value >= 1.0)) return fail(h, BES_ERR_ARGUMENT, "SolverOption: BiCG iterations must be >= 1");
             h->bicg_max_iter = (int)value;
             break;
-        case BES_OPT_WARPS_PER_BLOCK: h->warps_per_block = (int)value; break;
+        case BES_OPT_WARPS_PER_BLOCK:
+            h->warps_per_block = (int)value;
+            for (int c = 0; c < 3; c++) h->tuned_wpb[c] = 0;   /* an explicit shape replaces the tuned one */
+            break;
         case BES_OPT_USE_CUDA_GRAPH: h->use_graph = value != 0.0; break;
         case BES_OPT_WARPS_PER_SYSTEM:
             if (!(value == 0.0 || value == 1.0))
                 return fail(h, BES_ERR_ARGUMENT, "SolverOption: WarpsPerSystem must be 0 (automatic) or 1");
             h->warps_per_system = (int)value;
+            for (int c = 0; c < 3; c++) h->tuned_wps[c] = -1;
             break;
         default:
             return fail(h, BES_ERR_OPTION, "SolverOption: option %d needs an index argument or is not applicable", option);
@@ -1043,6 +1055,101 @@ bes_status bes_solve_periods(bes_solver* h, int32_t n_periods, int32_t reset_at)
 }
 
 bes_status bes_solve(bes_solver* h) { return bes_solve_periods(h, 1, -1); }
+
+/* Launch-shape autotuner: for every non-empty size class, time each launch
+ * shape the kernels allow (warps per system, then warps per CTA in powers of
+ * two up to what shared memory and the launch bounds admit) on the device's
+ * current inputs, from the same saved state each time, and keep the fastest.
+ * Every shape computes bit-identical results, so the choice changes speed
+ * only.  The state, accessories, dense output and counters on the device are
+ * restored afterwards; the host mirrors are not touched. */
+bes_status bes_autotune(bes_solver* h, int32_t n_periods, int64_t step_cap, bes_autotune_result* result) {
+    bes_status st = check_solver(h);
+    if (st) return st;
+    if (!result) return fail(h, BES_ERR_ARGUMENT, "bes_autotune: result is NULL");
+    std::memset(result, 0, sizeof(*result));
+    if (n_periods < 1) n_periods = 1;
+    if (h->order_dirty && (st = build_order(h))) return st;
+    const int saved[] = {B_TIME_DOMAIN, B_ACTUAL_TIME, B_STATE, B_UACC, B_IUACC, B_SACC, B_ISACC, B_DENSE_INDEX,
+                         B_DENSE_TIME, B_DENSE_STATE, B_CNT_ACC, B_CNT_REJ, B_CNT_BICG, B_CNT_RHS, B_STATUS};
+    constexpr int NSAVED = sizeof(saved) / sizeof(saved[0]);
+    void* backup[NSAVED] = {};
+    auto release = [&]() {
+        for (void*& p : backup)
+            if (p) { cudaFree(p); p = nullptr; }
+    };
+    auto restore = [&]() -> cudaError_t {
+        for (int k = 0; k < NSAVED; k++) {
+            const Buf& b = h->buf[saved[k]];
+            if (b.count <= 0) continue;
+            cudaError_t e = cudaMemcpyAsync(b.d, backup[k], b.bytes(), cudaMemcpyDeviceToDevice, h->stream);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    };
+    for (int k = 0; k < NSAVED; k++) {
+        const Buf& b = h->buf[saved[k]];
+        if (b.count <= 0) continue;
+        cudaError_t e = cudaMalloc(&backup[k], b.bytes());
+        if (e == cudaSuccess) e = cudaMemcpyAsync(backup[k], b.d, b.bytes(), cudaMemcpyDeviceToDevice, h->stream);
+        if (e != cudaSuccess) {
+            release();
+            return fail(h, BES_ERR_MEMORY, "bes_autotune: saving the device state: %s", cudaGetErrorString(e));
+        }
+    }
+    DeviceProblem P = make_problem(h);
+    P.n_periods = n_periods;
+    P.reset_at = -1;
+    if (step_cap > 0) P.max_steps_per_period = std::min<int64_t>(P.max_steps_per_period, step_cap);
+    for (int cls = 0; cls < 3 && !st; cls++) {
+        if (h->class_count[cls] == 0) continue;
+        float best = -1.0f;
+        int best_wps = 0, best_wpb = 0;
+        for (int wps = 0; wps <= (cls == 0 ? 0 : 1) && !st; wps++) {
+            const bes::Variant v = bes::class_variant(cls, h->class0_all32,
+                                                      h->shared_coupling && h->class_shared[cls], wps);
+            const int cap = bes::max_warps_per_block(v);
+            for (int wpb = v.G; wpb <= cap && !st; wpb *= 2) {
+                ClassLaunch L;
+                if ((st = plan_shape(h, cls, wps, wpb, &L))) break;
+                if (L.wpb != wpb) continue;   /* clamped to a shape already timed */
+                DeviceProblem Pc = P;
+                Pc.order = h->d_order + h->class_begin[cls];
+                Pc.n_active = h->class_count[cls];
+                Pc.work_counter = h->d_work + cls;
+                cudaError_t e = restore();
+                if (e == cudaSuccess) e = cudaMemsetAsync(h->d_work, 0, sizeof(int32_t) * 4, h->stream);
+                if (e == cudaSuccess) e = cudaEventRecord(h->t0, h->stream);
+                if (e == cudaSuccess) e = bes::launch(L.v, Pc, L.grid, L.wpb, h->stream);
+                if (e == cudaSuccess) e = cudaEventRecord(h->t1, h->stream);
+                if (e == cudaSuccess) e = cudaEventSynchronize(h->t1);
+                float ms = 0.0f;
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, h->t0, h->t1);
+                if (e != cudaSuccess) {
+                    st = fail(h, BES_ERR_CUDA, "bes_autotune: class %d, %d warps per system, %d per CTA: %s", cls,
+                              wps, wpb, cudaGetErrorString(e));
+                    break;
+                }
+                result->candidates++;
+                if (best < 0.0f || ms < best) { best = ms; best_wps = wps; best_wpb = L.wpb; }
+            }
+        }
+        if (!st) {
+            h->tuned_wps[cls] = best_wps;
+            h->tuned_wpb[cls] = best_wpb;
+            result->warps_per_system[cls] = best_wps;
+            result->warps_per_block[cls] = best_wpb;
+            result->ms[cls] = best;
+        }
+    }
+    cudaError_t e = restore();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    release();
+    h->graph_dirty = true;
+    if (st) return st;
+    if (e != cudaSuccess) return fail(h, BES_ERR_CUDA, "bes_autotune: restoring the device state: %s", cudaGetErrorString(e));
+    return BES_OK;
+}
 
 bes_status bes_synchronise_device(bes_solver* h) {
     bes_status st = check_solver(h);

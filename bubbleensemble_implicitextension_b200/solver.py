@@ -141,6 +141,11 @@ class CountersStruct(ctypes.Structure):
     ]
 
 
+class AutotuneResult(ctypes.Structure):
+    _fields_ = [("warps_per_block", ctypes.c_int32 * 3), ("warps_per_system", ctypes.c_int32 * 3),
+                ("ms", ctypes.c_float * 3), ("candidates", ctypes.c_int32)]
+
+
 class MlpConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("n_in", ctypes.c_int32), ("width", ctypes.c_int32),
                 ("depth", ctypes.c_int32), ("n_out", ctypes.c_int32), ("max_batch", ctypes.c_int32),
@@ -173,6 +178,7 @@ class NoallocProblem(ctypes.Structure):
 _I32, _D, _P = ctypes.c_int32, ctypes.c_double, ctypes.c_void_p
 _DP = ctypes.POINTER(ctypes.c_double)
 SIGNATURES = {
+    "bes_autotune": [_P, _I32, ctypes.c_int64, ctypes.POINTER(AutotuneResult)],
     "bes_create": [ctypes.POINTER(_Config), ctypes.POINTER(ctypes.c_void_p)],
     "bes_destroy": [_P],
     "bes_model_info_get": [ctypes.POINTER(ModelInfo)],
@@ -488,6 +494,14 @@ class ProblemSolver:
         ms = ctypes.c_float()
         self._ok(self._lib.bes_last_solve_ms(self._h, ctypes.byref(ms)))
         return ms.value
+
+    def autotune(self, n_periods: int = 1, step_cap: int = 2000) -> dict:
+        """Time every launch shape per size class on the device's current inputs
+        and keep the fastest (bes_autotune); the device state is restored."""
+        r = AutotuneResult()
+        self._ok(self._lib.bes_autotune(self._h, n_periods, step_cap, ctypes.byref(r)))
+        return {"warps_per_block": list(r.warps_per_block), "warps_per_system": list(r.warps_per_system),
+                "ms": [float(x) for x in r.ms], "candidates": int(r.candidates)}
 
     def last_solve_launches(self) -> int:
         n = ctypes.c_int32()

@@ -264,6 +264,22 @@ bes_status bes_device_info_get(int32_t device, bes_device_info* out);
  * denominator of the FP64 solver kernel. */
 bes_status bes_measure_fp64_peak(int32_t device, double* tflops);
 
+/* ---- launch-shape autotuner (no reference counterpart; the reference fixes
+ * threads and systems per block at compile time, Interface.cuh:135-248) ----
+ * Times every launch shape of every non-empty size class on the device's
+ * current inputs (n_periods periods, each system's attempted steps capped at
+ * step_cap per period when step_cap > 0), keeps the fastest per class for the
+ * following solves and restores the device state it started from.  Shapes
+ * give bit-identical results.  Setting BES_OPT_WARPS_PER_BLOCK or
+ * BES_OPT_WARPS_PER_SYSTEM afterwards replaces the tuned choice. */
+typedef struct bes_autotune_result {
+    int32_t warps_per_block[3];    /* per size class (N <= 32, <= 64, <= 128); 0 where the class is empty */
+    int32_t warps_per_system[3];   /* 0: 2 or 4 warps per system above 32 units, 1: one warp */
+    float ms[3];                   /* device time of the chosen shape */
+    int32_t candidates;            /* shapes timed in all */
+} bes_autotune_result;
+bes_status bes_autotune(bes_solver* h, int32_t n_periods, int64_t step_cap, bes_autotune_result* result);
+
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory: an application that already owns the GPU's memory (a framework that
  * reserves the device and hands out slices of its own pool, or a real-time

@@ -10,7 +10,7 @@ O = S.ListOfSolverOptions
 
 def run_gpu(ens, n_periods=None, reset_at=None, algorithm=S.Algorithms.RKCK45, ndo=0, do_min_dt=0.0,
             do_save_frequency=1, per_period_solve=False, warps_per_block=0, bicg_max_iter=19, use_graph=True,
-            repeat=1, shared_matrices=False, warps_per_system=0):
+            repeat=1, shared_matrices=False, warps_per_system=0, autotune=False):
     n_periods = ens.n_periods if n_periods is None else n_periods
     reset_at = ens.reset_at if reset_at is None else reset_at
     ps = ens.make_solver(algorithm=algorithm, n_dense_output=ndo)
@@ -33,6 +33,9 @@ def run_gpu(ens, n_periods=None, reset_at=None, algorithm=S.Algorithms.RKCK45, n
             ps.solve_periods(n_periods, reset_at)
             ps.reset_counters()
         ps.SynchroniseFromHostToDevice(V.All)
+        if autotune:
+            out_tune = ps.autotune(n_periods=1, step_cap=300)
+            assert out_tune["candidates"] >= 1
         if per_period_solve:
             for p in range(n_periods):
                 if p == reset_at:

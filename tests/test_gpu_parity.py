@@ -149,3 +149,12 @@ def test_coupling_factors_need_the_shared_matrix_kernels(gpu):
             ps.solve_periods(1, -1)
     finally:
         ps.close()
+
+
+def test_autotuned_shapes_give_identical_results(gpu):
+    """bes_autotune times every launch shape of every class, restores the device
+    state and keeps the fastest: the following solve equals a plain one."""
+    ens = bounded(ragged_ensemble([16, 32, 48, 64, 100, 128, 8, 40, 90, 20], seed=51))
+    a = run_gpu(ens, n_periods=1, reset_at=-1)
+    b = run_gpu(ens, n_periods=1, reset_at=-1, autotune=True)
+    assert_bitwise(b, a, KEYS)
