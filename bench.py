@@ -101,6 +101,9 @@ def parse():
     ap.add_argument("--sweep-spread", type=float, default=0.05)
     ap.add_argument("--sweep-disagreement", type=float, default=0.02)
     ap.add_argument("--sweep-dump", type=str, default="", help="c5_sweep: write the maps to this .npz")
+    ap.add_argument("--ref-regcap", choices=["capped", "uncapped"], default="uncapped",
+                    help="reference arm: the reference built without its shipped -maxrregcount=128 (the faster of "
+                         "the two on the B200: 44.8 vs 30.0 system-periods/s on c1_period1) or with it")
     ap.add_argument("--autotune", type=int, default=1, choices=[0, 1],
                     help="1: pick launch shapes with bes_autotune before the warm-up (untimed)")
     ap.add_argument("--warps-per-system", type=int, default=0, choices=[0, 1],
@@ -369,7 +372,7 @@ def run_reference(args, rank, world):
     from bubbleensemble_implicitextension_b200 import workloads as W
     from oracle import build_ref, ref_io
 
-    exe = build_ref.path(32, 256, 0, True)
+    exe = build_ref.path(32, 256, 0, args.ref_regcap == "capped")
     if not exe.exists():
         return {"impl": "reference", "unavailable": f"{exe.name} was not built (the reference tree was absent at build time)"}
     ens = W.c1_ensemble(n_periods=1, reset_at=-1)
@@ -390,7 +393,8 @@ def run_reference(args, rank, world):
                    "parallelism": "reference ProblemSolver, one GPU"},
         "cpu_baseline": {"value": value, "unit": UNIT, "kind": "reference", "cores": 1,
                          "sample": "the reference's own per-block CUDA solver (ProblemSolver<256,32,...,RKCK45,double>, "
-                                   "unmodified headers, nvcc -O3 -maxrregcount=128 sm_100a) on the same GPU, "
+                                   "unmodified headers, nvcc -O3 sm_100a, " + ("-maxrregcount=128 as shipped"
+                                   if args.ref_regcap == "capped" else "without the shipped register cap") + ") on the same GPU, "
                                    "timed per Solve() with the host thread waiting on its event; the reference "
                                    "has no CPU implementation"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
