@@ -72,7 +72,8 @@ constexpr unsigned FULL = 0xffffffffu;
  * shared-memory operator, the system's coupling matrix C with the
  * register-resident operator), six broadcast vectors, the group's exchange
  * buffers (G > 1), the system-scope arrays and (U = G = 1 only) the unit
- * parameters of the register-resident operator. */
+ * parameters of the register-resident operator and its operator W itself
+ * (column-major, ld NMAX+1: its columns feed the transposed product). */
 template <int U, int G = 1>
 struct WarpSmem {
     static constexpr int NMAX = 32 * U * G;
@@ -82,9 +83,11 @@ struct WarpSmem {
     static constexpr int XCH_DOUBLES = G > 1 ? 4 * NMAX : 0; /* two buffers of two values per unit */
     static constexpr int SYS_DOUBLES = NSPa + NSAa + NISAa;  /* ints stored in double slots */
     static constexpr int UP_DOUBLES = U == 1 && G == 1 ? NMAX * NUPa : 0; /* unit parameters, lane-contiguous */
+    static constexpr int WT_DOUBLES = U == 1 && G == 1 ? NMAX * LDW : 0;  /* operator W of the register variants */
     /* per-system stride rounded up to 256 bytes: every system's vectors stay
      * 16-byte aligned for the double2 broadcast loads */
-    static constexpr int DOUBLES = (W_DOUBLES + VEC_DOUBLES + XCH_DOUBLES + SYS_DOUBLES + UP_DOUBLES + 31) / 32 * 32;
+    static constexpr int DOUBLES =
+        (W_DOUBLES + WT_DOUBLES + VEC_DOUBLES + XCH_DOUBLES + SYS_DOUBLES + UP_DOUBLES + 31) / 32 * 32;
     static constexpr int BYTES = DOUBLES * 8;
     static_assert(DOUBLES % 2 == 0 && W_DOUBLES % 2 == 0 && NMAX % 2 == 0,
                   "broadcast vectors must start on 16-byte boundaries");
@@ -481,8 +484,10 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U, G>& S, const DeviceProbl
 
 /* ---------------------------------------------------------------------------
  * Coupled right-hand side with the operator in registers (N <= 32, one unit
- * per lane).  Lane i holds row i of W (for A p) and column i of W (for
- * A^T p~) as 64 doubles; the system's coupling matrix sits in shared memory
+ * per lane).  Lane i holds row i of W (for A p) in 32 registers and writes it
+ * to shared memory, from where it reads column i of W (for A^T p~; holding
+ * the column in registers as well cost 27 % of the step time on the B200 at
+ * 254 registers per thread); the system's coupling matrix sits in shared memory
  * (padded, leading dimension 33: row and column reads are conflict-free),
  * staged once per system.  NFIX = 32 drops the N guards for full warps.
  * Same arithmetic, in the same order, as the shared-memory variant. */
@@ -516,14 +521,13 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
     S.vxu[i] = xu;
     S.vrd[i] = rd;
     __syncwarp();
-    double wr[32], wc[32];
+    double wr[32];
     double bs[4] = {0.0, 0.0, 0.0, 0.0}, as[4] = {0.0, 0.0, 0.0, 0.0};
     const double* Crow = S.W + i;        /* C[i][j] at i + j*LDC */
-    const double* Ccol = S.W + i * LDC;  /* C[j][i] at j + i*LDC */
+    double* Wt = S.W + 32 * LDC;         /* W[i][j] at i + j*LDC, after the staged C */
 #pragma unroll
     for (int j = 0; j < 32; j++) {
         const double cij = Crow[j * LDC];
-        const double cji = Ccol[j];
         const double x1j = S.vx1[j];
         const bool in = NFIX != 0 || j < N;
         if (in) {
@@ -531,8 +535,10 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
             as[j & 3] = fma(cij * x1j, S.vxu[j], as[j & 3]);
         }
         wr[j] = in ? (rd * cij) * x1j : 0.0;
-        wc[j] = in ? (S.vrd[j] * cji) * x1 : 0.0;
     }
+#pragma unroll
+    for (int j = 0; j < 32; j++) Wt[j * LDC + i] = wr[j];
+    __syncwarp();
     double r = 0.0;
     if (valid) {
         const double b = fma(rd, (bs[0] + bs[1]) + (bs[2] + bs[3]), xu);
@@ -569,13 +575,15 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
             if (NFIX != 0 || j + 1 < N) qs[(j + 1) & 3] = fma(wr[j + 1], a.y, qs[(j + 1) & 3]);
         }
         double q = p + ((qs[0] + qs[1]) + (qs[2] + qs[3]));
-        /* first tree level t_k + t_{k+16} on the loads, then the halving tree over 16 */
+        /* column i of W from shared memory (lane-consecutive rows, conflict-free);
+         * first tree level t_k + t_{k+16} on the loads, then the halving tree over 16 */
+        const double* Wc = Wt + i * LDC;
         double u[16];
 #pragma unroll
         for (int k = 0; k < 16; k += 2) {
             const double2 lo = vpt2[k / 2], hi = vpt2[(k + 16) / 2];
-            u[k] = wc[k] * lo.x + wc[k + 16] * hi.x;
-            u[k + 1] = wc[k + 1] * lo.y + wc[k + 17] * hi.y;
+            u[k] = Wc[k] * lo.x + Wc[k + 16] * hi.x;
+            u[k + 1] = Wc[k + 1] * lo.y + Wc[k + 17] * hi.y;
         }
         auto leaf = [&](int k) -> double { return u[k]; };
         double qt = pt + TreeSum<1, 16>::run(0, leaf);
@@ -1293,7 +1301,7 @@ __global__ void __launch_bounds__(RHS == 3 || G > 1 ? 256 : 128, 1) bes_ensemble
         using SM = WarpSmem<U, G>;
         double* base = smem + (size_t)slot * SM::DOUBLES;
         S.W = base;
-        S.vp = base + SM::W_DOUBLES;
+        S.vp = base + SM::W_DOUBLES + SM::WT_DOUBLES;
         S.vpt = S.vp + SM::NMAX;
         S.vcpt = S.vpt + SM::NMAX;
         S.vx1 = S.vcpt + SM::NMAX;
