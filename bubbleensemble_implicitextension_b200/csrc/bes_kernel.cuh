@@ -71,8 +71,9 @@ constexpr unsigned FULL = 0xffffffffu;
  * units): one NMAX x (NMAX+1) matrix region (the operator W with the
  * shared-memory operator, the system's coupling matrix C with the
  * register-resident operator), six broadcast vectors, the group's exchange
- * buffers (G > 1), the system-scope arrays and (U = G = 1 only) the unit
- * parameters of the register-resident operator and its operator W itself
+ * buffers (G > 1), the system-scope arrays, the unit parameters when each
+ * lane owns one unit (U = 1: in registers they crowd out the BiCG state) and
+ * for the register-resident operator (U = G = 1) the operator W itself
  * (column-major, ld NMAX+1: its columns feed the transposed product). */
 template <int U, int G = 1>
 struct WarpSmem {
@@ -82,7 +83,7 @@ struct WarpSmem {
     static constexpr int VEC_DOUBLES = 6 * NMAX;
     static constexpr int XCH_DOUBLES = G > 1 ? 4 * NMAX : 0; /* two buffers of two values per unit */
     static constexpr int SYS_DOUBLES = NSPa + NSAa + NISAa;  /* ints stored in double slots */
-    static constexpr int UP_DOUBLES = U == 1 && G == 1 ? NMAX * NUPa : 0; /* unit parameters, lane-contiguous */
+    static constexpr int UP_DOUBLES = U == 1 ? NMAX * NUPa : 0; /* unit parameters (one unit per lane) */
     static constexpr int WT_DOUBLES = U == 1 && G == 1 ? NMAX * LDW : 0;  /* operator W of the register variants */
     /* per-system stride rounded up to 256 bytes: every system's vectors stay
      * 16-byte aligned for the double2 broadcast loads */
@@ -104,7 +105,8 @@ struct SharedCSmem {
     static constexpr int LDC = NMAX + 2;
     static constexpr int C_DOUBLES = NMAX * LDC;
     static constexpr int XCH_DOUBLES = G > 1 ? 4 * NMAX : 0;
-    static constexpr int WARP_DOUBLES = (5 * NMAX + XCH_DOUBLES + NSPa + NSAa + NISAa + 31) / 32 * 32;
+    static constexpr int UP_DOUBLES = U == 1 ? NMAX * NUPa : 0; /* unit parameters (one unit per lane) */
+    static constexpr int WARP_DOUBLES = (5 * NMAX + XCH_DOUBLES + NSPa + NSAa + NISAa + UP_DOUBLES + 31) / 32 * 32;
     static constexpr int C_BYTES = C_DOUBLES * 8;
     static constexpr int WARP_BYTES = WARP_DOUBLES * 8;
     static_assert(LDC % 2 == 0 && C_DOUBLES % 2 == 0 && WARP_DOUBLES % 2 == 0, "16-byte alignment");
@@ -346,7 +348,8 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U, G>& S, const DeviceProbl
         const int i = S.unit(m);
         if (i < N) {
             double Fl[UD], cpt, cpf;
-            CoupledSystems_PerBlock_OdeFunction<double>(S.sid, i, Fl, Xs[m], T, up[m], S.sPAR, S.gPAR, S.igPAR,
+            CoupledSystems_PerBlock_OdeFunction<double>(S.sid, i, Fl, Xs[m], T, U == 1 ? S.upsh + i * NUPa : up[m],
+                                                        S.sPAR, S.gPAR, S.igPAR,
                                                         ua[m], iua[m], S.sACC, S.isACC, &cpt, &cpf);
 #pragma unroll
             for (int k = 0; k < UD; k++) F[m][k] = Fl[k];
@@ -636,7 +639,8 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const Dev
         const int i = S.unit(m);
         if (i < N) {
             double Fl[UD], cpt, cpf;
-            CoupledSystems_PerBlock_OdeFunction<double>(S.sid, i, Fl, Xs[m], T, up[m], S.sPAR, S.gPAR, S.igPAR,
+            CoupledSystems_PerBlock_OdeFunction<double>(S.sid, i, Fl, Xs[m], T, U == 1 ? S.upsh + i * NUPa : up[m],
+                                                        S.sPAR, S.gPAR, S.igPAR,
                                                         ua[m], iua[m], S.sACC, S.isACC, &cpt, &cpf);
 #pragma unroll
             for (int k = 0; k < UD; k++) F[m][k] = Fl[k];
@@ -823,7 +827,7 @@ __device__ __forceinline__ bool valid_unit(const Sys<U, G>& S, int m) { return S
 /* the parameter array a callback gets for slot m of this lane */
 template <int U, int RHS, int G>
 __device__ __forceinline__ double* upar_of(const Sys<U, G>& S, Lane<U>& L, int m) {
-    if constexpr (RHS == 1 || RHS == 2) return S.upsh + (S.unit(m)) * NUPa;
+    if constexpr (U == 1) return S.upsh + (S.unit(m)) * NUPa;
     else return L.up[m];
 }
 
@@ -1296,7 +1300,7 @@ __global__ void __launch_bounds__(RHS == 3 || G > 1 ? 256 : 128, 1) bes_ensemble
         S.vrd = nullptr;
         S.xch = base + 5 * NM;
         S.sPAR = S.xch + SM::XCH_DOUBLES;
-        S.upsh = nullptr;
+        S.upsh = S.sPAR + NSPa + NSAa + NISAa;
     } else {
         using SM = WarpSmem<U, G>;
         double* base = smem + (size_t)slot * SM::DOUBLES;
@@ -1342,7 +1346,7 @@ __global__ void __launch_bounds__(RHS == 3 || G > 1 ? 256 : 128, 1) bes_ensemble
             const int64_t g = S.off + i;
 #pragma unroll
             for (int c = 0; c < UD; c++) L.X[m][c] = v ? P.state[(int64_t)c * S.tot + g] : 0.0;
-            if constexpr (RHS == 1 || RHS == 2) {
+            if constexpr (U == 1) {
                 for (int c = 0; c < NUP; c++) S.upsh[i * NUPa + c] = v ? __ldg(P.upar + (int64_t)c * S.tot + g) : 0.0;
             } else {
 #pragma unroll
