@@ -16,6 +16,8 @@
 
 #include <algorithm>
 #include <cerrno>
+#include <fstream>
+#include <ios>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -41,7 +43,9 @@ namespace {
 enum BufId {
     B_TIME_DOMAIN, B_ACTUAL_TIME, B_STATE, B_UPAR, B_SPAR, B_GPAR, B_IGPAR, B_UACC, B_IUACC, B_SACC, B_ISACC,
     B_COUPLING, B_COUPLING_STRENGTH, B_COUPLING_INDEX, B_DENSE_INDEX, B_DENSE_TIME, B_DENSE_STATE,
-    B_RTOL, B_ATOL, B_CROW, B_CCOL, B_CNT_ACC, B_CNT_REJ, B_CNT_BICG, B_CNT_RHS, B_STATUS, B_COUNT
+    B_RTOL, B_ATOL, B_CROW, B_CCOL, B_CNT_ACC, B_CNT_REJ, B_CNT_BICG, B_CNT_RHS, B_STATUS,
+    B_PREF, B_PERIOD, B_MAXACC, B_POINCARE,   /* period analysis, allocated by bes_set_period_analysis */
+    B_COUNT
 };
 
 struct Buf {
@@ -90,6 +94,9 @@ struct bes_solver {
     long long max_steps = 1000000;
     /* launch plan */
     bool order_dirty = true;
+    int analysis_sections = -1;   /* -1: per-period analysis off */
+    double analysis_tol = 1e-6;
+    int analysis_accessory = 0;
     bool scaled_coupling[2] = {false, false};   /* a host copy of CouplingRow/ColumnScale with a value != 1 went to the device */
     int class_begin[3] = {0, 0, 0}, class_count[3] = {0, 0, 0};
     bool class0_all32 = false;
@@ -133,7 +140,7 @@ bes_status fail(bes_solver* h, bes_status code, const char* fmt, ...) {
 
 bool is_int_buf(int id) {
     return id == B_IGPAR || id == B_IUACC || id == B_ISACC || id == B_COUPLING_INDEX || id == B_DENSE_INDEX ||
-           id == B_STATUS;
+           id == B_STATUS || id == B_PERIOD;
 }
 
 int var_to_buf(int var) {
@@ -159,6 +166,9 @@ int var_to_buf(int var) {
         case BES_ABSOLUTE_TOLERANCE_SYSTEM: return B_ATOL;
         case BES_COUPLING_ROW_SCALE: return B_CROW;
         case BES_COUPLING_COLUMN_SCALE: return B_CCOL;
+        case BES_POINCARE_SECTIONS: return B_POINCARE;
+        case BES_PERIOD_NUMBER: return B_PERIOD;
+        case BES_MAXIMUM_ACCESSORY: return B_MAXACC;
         default: return -1;
     }
 }
@@ -189,6 +199,9 @@ const char* var_name(int var) {
         case BES_COUNTERS: return "Counters";
         case BES_COUPLING_ROW_SCALE: return "CouplingRowScale";
         case BES_COUPLING_COLUMN_SCALE: return "CouplingColumnScale";
+        case BES_POINCARE_SECTIONS: return "PoincareSections";
+        case BES_PERIOD_NUMBER: return "PeriodNumber";
+        case BES_MAXIMUM_ACCESSORY: return "MaximumAccessory";
         default: return "unknown";
     }
 }
@@ -301,6 +314,15 @@ DeviceProblem make_problem(bes_solver* h) {
     P.actual_time = (double*)h->buf[B_ACTUAL_TIME].d;
     P.rtol = (const double*)h->buf[B_RTOL].d;
     P.coupling_row_scale = (const double*)h->buf[B_CROW].d;
+    if (h->analysis_sections >= 0) {
+        P.period_ref = (double*)h->buf[B_PREF].d;
+        P.period_number = (int32_t*)h->buf[B_PERIOD].d;
+        P.period_tol = h->analysis_tol;
+        P.max_accessory = (double*)h->buf[B_MAXACC].d;
+        P.max_accessory_index = h->analysis_accessory;
+        P.n_sections = h->analysis_sections;
+        P.poincare = h->analysis_sections > 0 ? (double*)h->buf[B_POINCARE].d : nullptr;
+    }
     P.coupling_col_scale = (const double*)h->buf[B_CCOL].d;
     P.atol = (const double*)h->buf[B_ATOL].d;
     P.event_tol = h->d_event_tol;
@@ -1055,6 +1077,122 @@ bes_status bes_solve_periods(bes_solver* h, int32_t n_periods, int32_t reset_at)
 }
 
 bes_status bes_solve(bes_solver* h) { return bes_solve_periods(h, 1, -1); }
+
+/* ---------------- per-period analysis and output files ---------------- */
+
+bes_status bes_set_period_analysis(bes_solver* h, int32_t sections, double distance_tolerance,
+                                   int32_t accessory_index) {
+    bes_status st = check_solver(h);
+    if (st) return st;
+    if (sections >= 0 && !(distance_tolerance >= 0.0))
+        return fail(h, BES_ERR_ARGUMENT, "bes_set_period_analysis: distance tolerance must be >= 0");
+    if (sections >= 0 && (accessory_index < 0 || accessory_index >= std::max(1, h->nua)))
+        return fail(h, BES_ERR_INDEX, "bes_set_period_analysis: accessory index %d out of range (0-%d)",
+                    accessory_index, std::max(1, h->nua) - 1);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    for (int id : {B_PREF, B_PERIOD, B_MAXACC, B_POINCARE}) {
+        Buf& b = h->buf[id];
+        if (b.h) cudaFreeHost(b.h);
+        if (b.d) cudaFree(b.d);
+        b.h = b.d = nullptr;
+        b.count = 0;
+    }
+    h->analysis_sections = -1;
+    h->graph_dirty = true;
+    if (sections < 0) return BES_OK;
+    const int64_t TU = h->total_units;
+    const struct { int id; int64_t count; } sizes[] = {
+        {B_PREF, h->ud * TU}, {B_PERIOD, TU}, {B_MAXACC, TU}, {B_POINCARE, (int64_t)sections * TU}};
+    for (auto& sz : sizes) {
+        Buf& b = h->buf[sz.id];
+        b.count = sz.count;
+        b.elem = is_int_buf(sz.id) ? 4 : 8;
+        if (b.count <= 0) continue;
+        cudaError_t e = cudaMallocHost(&b.h, b.bytes());
+        if (e == cudaSuccess) e = cudaMalloc(&b.d, b.bytes());
+        if (e == cudaSuccess) e = cudaMemsetAsync(b.d, 0, b.bytes(), h->stream);
+        if (e != cudaSuccess) {
+            bes_set_period_analysis(h, -1, 0.0, 0);
+            return fail(h, BES_ERR_MEMORY, "bes_set_period_analysis: %lld sections of %lld units: %s",
+                        (long long)sections, (long long)TU, cudaGetErrorString(e));
+        }
+        std::memset(b.h, 0, b.bytes());
+    }
+    h->analysis_sections = sections;
+    h->analysis_tol = distance_tolerance;
+    h->analysis_accessory = accessory_index;
+    return BES_OK;
+}
+
+/* The reference drivers' output files, written from the host mirrors (call
+ * bes_synchronise_device_to_host for the variables first):
+ *   BES_CSV_COLLAPSE   CollapseStrength.cu:174-198  (per system and record slot: id, uPAR15, uPAR16,
+ *                      every unit's uACC[slot], every unit's uACC[slot + NUA/2])
+ *   BES_CSV_POINCARE   BubbleEnsemble.cu:435-455    (per stored section and system: id, uPAR15, R/R_E per unit)
+ *   BES_CSV_PERIOD     BubbleEnsemble.cu:457-473    (per system: id, uPAR15, period number per unit)
+ *   BES_CSV_EXPANSION  BubbleEnsemble.cu:475-491    (per system: id, uPAR16, the maximum accessory per unit,
+ *                      truncated to an integer as the reference's int array stores it)
+ * with the reference's stream widths, precisions and scientific notation. */
+bes_status bes_write_csv(bes_solver* h, int32_t kind, const char* path) {
+    bes_status st = check_solver(h);
+    if (st) return st;
+    if (!path) return fail(h, BES_ERR_ARGUMENT, "bes_write_csv: path is NULL");
+    if (h->nup < 17) return fail(h, BES_ERR_MODEL, "bes_write_csv: the system definition has fewer than 17 unit parameters");
+    if ((kind == BES_CSV_POINCARE || kind == BES_CSV_PERIOD || kind == BES_CSV_EXPANSION) && h->analysis_sections < 0)
+        return fail(h, BES_ERR_ARGUMENT, "bes_write_csv: per-period analysis is off (bes_set_period_analysis)");
+    if (kind == BES_CSV_COLLAPSE && (h->nua < 2 || h->nua % 2))
+        return fail(h, BES_ERR_MODEL, "bes_write_csv: the collapse file needs an even number of unit accessories");
+    if (kind < BES_CSV_COLLAPSE || kind > BES_CSV_EXPANSION)
+        return fail(h, BES_ERR_ARGUMENT, "bes_write_csv: unknown kind %d", kind);
+    std::ofstream f(path);
+    if (!f) return fail(h, BES_ERR_IO, "bes_write_csv: cannot open %s", path);
+    f.flags(std::ios::scientific);
+    const double* up = (const double*)h->buf[B_UPAR].h;
+    const int64_t TU = h->total_units;
+    auto upar = [&](int s, int k) { return up[(int64_t)k * TU + h->unit_offset[s]]; };
+    if (kind == BES_CSV_COLLAPSE) {
+        const double* ua = (const double*)h->buf[B_UACC].h;
+        const int ncoll = h->nua / 2;
+        for (int s = 0; s < h->n_systems; s++) {
+            const int64_t off = h->unit_offset[s];
+            for (int c = 0; c < ncoll; c++) {
+                f.width(6); f << s << ',';
+                f.width(17); f.precision(10); f << upar(s, 15) << ',';
+                f.width(17); f.precision(10); f << upar(s, 16) << ',';
+                for (int u = 0; u < h->units[s]; u++) {
+                    f.width(10); f.precision(3); f << ua[(int64_t)c * TU + off + u] << ',';
+                }
+                for (int u = 0; u < h->units[s]; u++) {
+                    f.width(10); f.precision(3); f << ua[(int64_t)(c + ncoll) * TU + off + u] << ',';
+                }
+                f << '\n';
+            }
+        }
+    } else {
+        f.precision(10);
+        const int W = 18;
+        const int nsec = kind == BES_CSV_POINCARE ? h->analysis_sections : 1;
+        for (int k = 0; k < nsec; k++) {
+            for (int s = 0; s < h->n_systems; s++) {
+                const int64_t off = h->unit_offset[s];
+                f.width(4); f << s << ',';
+                f.width(W); f << upar(s, kind == BES_CSV_EXPANSION ? 16 : 15) << ',';
+                for (int u = 0; u < h->units[s]; u++) {
+                    if (kind == BES_CSV_POINCARE) {
+                        f.width(W); f << ((const double*)h->buf[B_POINCARE].h)[(int64_t)k * TU + off + u] << ',';
+                    } else if (kind == BES_CSV_PERIOD) {
+                        f.width(4); f << ((const int32_t*)h->buf[B_PERIOD].h)[off + u] << ',';
+                    } else {
+                        f.width(4); f << (int)((const double*)h->buf[B_MAXACC].h)[off + u] << ',';
+                    }
+                }
+                f << '\n';
+            }
+        }
+    }
+    if (!f) return fail(h, BES_ERR_IO, "bes_write_csv: writing %s failed", path);
+    return BES_OK;
+}
 
 /* Launch-shape autotuner: for every non-empty size class, time each launch
  * shape the kernels allow (warps per system, then warps per CTA in powers of

@@ -66,6 +66,14 @@ struct DeviceProblem {
     int32_t reset_at;                /* period index before which accessories are reset (-1: never) */
     const double* uacc_reset;        /* [NUA] */
     const int32_t* iuacc_reset;      /* [NIUA] */
+    /* per-period analysis of a call (all NULL: off), after BubbleEnsemble.cu:174-216 */
+    double* period_ref;              /* [UD][total_units] the state at the call's start */
+    int32_t* period_number;          /* [total_units] first period (1-based) ending within period_tol of it, 0: none */
+    double period_tol;
+    double* max_accessory;           /* [total_units] running max of unit accessory max_accessory_index at period ends */
+    int32_t max_accessory_index;
+    int32_t n_sections;              /* Poincare sections stored per call */
+    double* poincare;                /* [n_sections][total_units] state component 0 at the end of each period */
 };
 
 }  // namespace bes

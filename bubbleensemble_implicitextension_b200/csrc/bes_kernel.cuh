@@ -1256,6 +1256,55 @@ __device__ void run_period(const Sys<U, G>& S, const DeviceProblem& P, Lane<U>& 
 }
 
 /* ---------------------------------------------------------------------------
+ * Per-period analysis (BubbleEnsemble.cu:174-216, moved onto the device): at
+ * the start of a call each unit's state is the reference point and the
+ * running maximum starts from the unit accessory; after every period the
+ * unit's state component 0 goes to that period's Poincare section, the first
+ * period whose end state lies within period_tol (Euclidean over the state
+ * components) of the reference point is recorded 1-based, and the maximum is
+ * raised when the accessory exceeds it.  Everything lives in HBM between
+ * periods, so nothing stays in registers across a period. */
+template <int U, int G>
+__device__ __forceinline__ void analysis_start(const Sys<U, G>& S, const DeviceProblem& P, const Lane<U>& L) {
+#pragma unroll
+    for (int m = 0; m < U; m++) {
+        const int i = S.unit(m);
+        if (i >= S.N) continue;
+        const int64_t g = S.off + i;
+#pragma unroll
+        for (int c = 0; c < UD; c++) P.period_ref[(int64_t)c * S.tot + g] = L.X[m][c];
+        P.period_number[g] = 0;
+        double a = 0.0;
+        for (int c = 0; c < NUA; c++)
+            if (c == P.max_accessory_index) a = L.ua[m][c];
+        P.max_accessory[g] = a;
+    }
+}
+
+template <int U, int G>
+__device__ __forceinline__ void analysis_period_end(const Sys<U, G>& S, const DeviceProblem& P, const Lane<U>& L,
+                                                    int per) {
+#pragma unroll
+    for (int m = 0; m < U; m++) {
+        const int i = S.unit(m);
+        if (i >= S.N) continue;
+        const int64_t g = S.off + i;
+        if (per < P.n_sections) P.poincare[(int64_t)per * S.tot + g] = L.X[m][0];
+        double d2 = 0.0;
+#pragma unroll
+        for (int c = 0; c < UD; c++) {
+            const double d = P.period_ref[(int64_t)c * S.tot + g] - L.X[m][c];
+            d2 = c == 0 ? d * d : d2 + d * d;   /* products rounded, then summed, in component order */
+        }
+        if (sqrt(d2) < P.period_tol && P.period_number[g] == 0) P.period_number[g] = per + 1;
+        double a = 0.0;
+        for (int c = 0; c < NUA; c++)
+            if (c == P.max_accessory_index) a = L.ua[m][c];
+        if (a > P.max_accessory[g]) P.max_accessory[g] = a;
+    }
+}
+
+/* ---------------------------------------------------------------------------
  * The kernel: groups of G warps pull systems from the work counter.
  * RHS = 0: operator W in shared memory; RHS = 1 / 2: operator in registers
  * (U = 1, G = 1; 2 = every system of the launch has exactly 32 units);
@@ -1382,6 +1431,7 @@ __global__ void __launch_bounds__(RHS == 3 || G > 1 ? 256 : 128, 1) bes_ensemble
         int do_idx = P.ndo > 0 ? P.dense_index[sid] : 0;
         grp_sync(S);
         Counters cnt = {0ull, 0ull, 0ull, 0ull, 0};
+        if (P.period_ref) analysis_start<U, G>(S, P, L);
         for (int per = 0; per < P.n_periods; per++) {
             if (per == P.reset_at) {
 #pragma unroll
@@ -1393,6 +1443,7 @@ __global__ void __launch_bounds__(RHS == 3 || G > 1 ? 256 : 128, 1) bes_ensemble
                 }
             }
             run_period<U, RHS, G>(S, P, L, cnt, TD, T, do_idx);
+            if (P.period_ref) analysis_period_end<U, G>(S, P, L, per);
         }
         /* write-back (Solver.cuh:599-648) */
         grp_sync(S);

@@ -49,6 +49,9 @@ class ListOfVariables(IntEnum):
     Counters = 102
     CouplingRowScale = 103
     CouplingColumnScale = 104
+    PoincareSections = 105
+    PeriodNumber = 106
+    MaximumAccessory = 107
 
 
 class ListOfSolverOptions(IntEnum):
@@ -91,7 +94,8 @@ STATUS_EVENT_MISSED = 8
 STATUS_BICG_CAP = 16
 
 _INT_VARS = {ListOfVariables.IntegerGlobalParameters, ListOfVariables.IntegerUnitAccessories,
-             ListOfVariables.IntegerSystemAccessories, ListOfVariables.CouplingIndex, ListOfVariables.DenseIndex}
+             ListOfVariables.IntegerSystemAccessories, ListOfVariables.CouplingIndex, ListOfVariables.DenseIndex,
+             ListOfVariables.PeriodNumber}
 
 LIB_PATH = Path(__file__).resolve().parent / "libbes.so"
 
@@ -141,6 +145,14 @@ class CountersStruct(ctypes.Structure):
     ]
 
 
+class CsvKind(IntEnum):
+    """bes_write_csv kinds: the reference drivers' output files."""
+    Collapse = 0     # CollapseStrength.cu:174-198
+    Poincare = 1     # BubbleEnsemble.cu:435-455
+    Period = 2       # BubbleEnsemble.cu:457-473
+    Expansion = 3    # BubbleEnsemble.cu:475-491
+
+
 class AutotuneResult(ctypes.Structure):
     _fields_ = [("warps_per_block", ctypes.c_int32 * 3), ("warps_per_system", ctypes.c_int32 * 3),
                 ("ms", ctypes.c_float * 3), ("candidates", ctypes.c_int32)]
@@ -179,6 +191,8 @@ _I32, _D, _P = ctypes.c_int32, ctypes.c_double, ctypes.c_void_p
 _DP = ctypes.POINTER(ctypes.c_double)
 SIGNATURES = {
     "bes_autotune": [_P, _I32, ctypes.c_int64, ctypes.POINTER(AutotuneResult)],
+    "bes_set_period_analysis": [_P, _I32, _D, _I32],
+    "bes_write_csv": [_P, _I32, ctypes.c_char_p],
     "bes_create": [ctypes.POINTER(_Config), ctypes.POINTER(ctypes.c_void_p)],
     "bes_destroy": [_P],
     "bes_model_info_get": [ctypes.POINTER(ModelInfo)],
@@ -494,6 +508,15 @@ class ProblemSolver:
         ms = ctypes.c_float()
         self._ok(self._lib.bes_last_solve_ms(self._h, ctypes.byref(ms)))
         return ms.value
+
+    def set_period_analysis(self, sections: int, distance_tolerance: float = 1e-6, accessory_index: int = 0) -> None:
+        """Per-period analysis of the following solves on the device (bes_set_period_analysis);
+        sections < 0 turns it off."""
+        self._ok(self._lib.bes_set_period_analysis(self._h, sections, distance_tolerance, accessory_index))
+
+    def write_csv(self, kind: int, path) -> None:
+        """One of the reference drivers' output files from the host mirrors (bes_write_csv)."""
+        self._ok(self._lib.bes_write_csv(self._h, kind, str(path).encode()))
 
     def autotune(self, n_periods: int = 1, step_cap: int = 2000) -> dict:
         """Time every launch shape per size class on the device's current inputs

@@ -74,6 +74,9 @@ typedef int32_t bes_status;
                                               (a_i = R_i^-2, b_j = R_j^3).  Applied by the shared-matrix
                                               kernels only (SharedCouplingMatrices, more than 32 units);
                                               a solve with other launches and factors != 1 is an error. */
+#define BES_POINCARE_SECTIONS 105          /* [sections][total_units] per-period analysis outputs (device -> host), */
+#define BES_PERIOD_NUMBER 106              /* [total_units] int32       see bes_set_period_analysis              */
+#define BES_MAXIMUM_ACCESSORY 107          /* [total_units]                                                       */
 
 /* ListOfSolverOptions, same names and order as Interface.cuh:55-68 */
 #define BES_OPT_INITIAL_TIME_STEP 0
@@ -263,6 +266,29 @@ bes_status bes_device_info_get(int32_t device, bes_device_info* out);
  * keeps 8 independent chains per thread on every SM; the roofline
  * denominator of the FP64 solver kernel. */
 bes_status bes_measure_fp64_peak(int32_t device, double* tflops);
+
+/* ---- per-period analysis on the device (BubbleEnsemble.cu:174-216 runs it on
+ * the host after every Solve()) ----
+ * sections >= 0 turns it on for the following bes_solve_periods calls: each
+ * call takes every unit's state at its start as the reference point, stores
+ * state component 0 after each of its first `sections` periods
+ * (BES_POINCARE_SECTIONS, [sections][total_units]), records the first period
+ * (1-based) whose end state lies within distance_tolerance of the reference
+ * point (Euclidean over the state components; BES_PERIOD_NUMBER, int32
+ * [total_units], 0: none) and the running maximum over period ends of unit
+ * accessory accessory_index, starting from its value at the call's start
+ * (BES_MAXIMUM_ACCESSORY, [total_units]).  The reference uses tolerance 1e-6
+ * and accessory 0.  sections < 0 turns it off and frees the arrays. */
+bes_status bes_set_period_analysis(bes_solver* h, int32_t sections, double distance_tolerance,
+                                   int32_t accessory_index);
+/* Output files of the reference drivers (CollapseStrength.cu:174-198,
+ * BubbleEnsemble.cu:435-491) from the host mirrors, same layout and number
+ * formats; kind is one of BES_CSV_*. */
+#define BES_CSV_COLLAPSE 0
+#define BES_CSV_POINCARE 1
+#define BES_CSV_PERIOD 2
+#define BES_CSV_EXPANSION 3
+bes_status bes_write_csv(bes_solver* h, int32_t kind, const char* path);
 
 /* ---- launch-shape autotuner (no reference counterpart; the reference fixes
  * threads and systems per block at compile time, Interface.cuh:135-248) ----
