@@ -224,7 +224,8 @@ class ProblemSolver {
         int64_t n = 0;
         bes_shim::check(bes_array_size(h_, Variable, &n), h_, "Print");
         const bool is_int = Variable == IntegerGlobalParameters || Variable == IntegerUnitAccessories ||
-                            Variable == IntegerSystemAccessories || Variable == CouplingIndex || Variable == DenseIndex;
+                            Variable == IntegerSystemAccessories || Variable == CouplingIndex || Variable == DenseIndex ||
+                            Variable == (ListOfVariables)BES_PERIOD_NUMBER;
         std::vector<double> d;
         std::vector<int32_t> iv;
         if (is_int) { iv.resize(n); bes_shim::check(bes_get_array(h_, Variable, iv.data(), n), h_, "Print"); }
@@ -248,6 +249,19 @@ class ProblemSolver {
     void Solve() { bes_shim::check(bes_solve(h_), h_, "Solve"); }
     /* extension: n_periods Solve() calls (accessories reset before period reset_at) in one launch */
     void SolvePeriods(int n_periods, int reset_at) { bes_shim::check(bes_solve_periods(h_, n_periods, reset_at), h_, "SolvePeriods"); }
+    /* extensions: per-period analysis on the device, the drivers' output files, launch-shape autotuning */
+    void SetPeriodAnalysis(int sections, double distance_tolerance = 1e-6, int accessory_index = 0) {
+        bes_shim::check(bes_set_period_analysis(h_, sections, distance_tolerance, accessory_index), h_,
+                        "SetPeriodAnalysis");
+    }
+    void WriteCSV(int kind, const std::string& path) {
+        bes_shim::check(bes_write_csv(h_, kind, path.c_str()), h_, "WriteCSV");
+    }
+    bes_autotune_result Autotune(int n_periods = 1, int64_t step_cap = 2000) {
+        bes_autotune_result r;
+        bes_shim::check(bes_autotune(h_, n_periods, step_cap, &r), h_, "Autotune");
+        return r;
+    }
     void SynchroniseDevice() { bes_shim::check(bes_synchronise_device(h_), h_, "SynchroniseDevice"); }
     void InsertSynchronisationPoint() {
         bes_shim::check(bes_insert_synchronisation_point(h_), h_, "InsertSynchronisationPoint");
