@@ -528,16 +528,25 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
     double bs[4] = {0.0, 0.0, 0.0, 0.0}, as[4] = {0.0, 0.0, 0.0, 0.0};
     const double* Crow = S.W + i;        /* C[i][j] at i + j*LDC */
     double* Wt = S.W + 32 * LDC;         /* W[i][j] at i + j*LDC, after the staged C */
+    /* the broadcast vectors are read two entries at a time (16-byte aligned) */
+    const double2* vx1_2 = reinterpret_cast<const double2*>(S.vx1);
+    const double2* vcpt2 = reinterpret_cast<const double2*>(S.vcpt);
+    const double2* vxu2 = reinterpret_cast<const double2*>(S.vxu);
 #pragma unroll
-    for (int j = 0; j < 32; j++) {
-        const double cij = Crow[j * LDC];
-        const double x1j = S.vx1[j];
-        const bool in = NFIX != 0 || j < N;
-        if (in) {
-            bs[j & 3] = fma(cij, S.vcpt[j], bs[j & 3]);
-            as[j & 3] = fma(cij * x1j, S.vxu[j], as[j & 3]);
+    for (int j = 0; j < 32; j += 2) {
+        const double2 x1p = vx1_2[j / 2], cpp = vcpt2[j / 2], xup = vxu2[j / 2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int jj = j + h;
+            const double cij = Crow[jj * LDC];
+            const double x1j = h ? x1p.y : x1p.x;
+            const bool in = NFIX != 0 || jj < N;
+            if (in) {
+                bs[jj & 3] = fma(cij, h ? cpp.y : cpp.x, bs[jj & 3]);
+                as[jj & 3] = fma(cij * x1j, h ? xup.y : xup.x, as[jj & 3]);
+            }
+            wr[jj] = in ? (rd * cij) * x1j : 0.0;
         }
-        wr[j] = in ? (rd * cij) * x1j : 0.0;
     }
 #pragma unroll
     for (int j = 0; j < 32; j++) Wt[j * LDC + i] = wr[j];

@@ -12,7 +12,8 @@
  *          Taylor polynomial, exponent-field scaling;
  *   log    x = 2^e m, m in (sqrt2/2, sqrt2], log(1+f) = f - s (f - T(s^2))
  *          with s = f/(2+f) and T the atanh series, kept as head + tail;
- *   pow    exp(y log x) with y*log x carried as head + tail;
+ *   pow    exp(y log x) with y*log x carried as head + tail (pow_recip:
+ *          (1/x)^y as exp(-y log x));
  *   sinpi  x = n/2 + r, |r| <= 1/4, Taylor series of sin(pi r), cos(pi r);
  *   sin    Cody-Waite reduction by pi/2 in three parts, Taylor series.
  * Coefficients are Taylor coefficients (1/k!, pi^k/k!, 2/(2k+1)) and digit
@@ -158,6 +159,20 @@ __device__ __forceinline__ double pow(double x, double y) {
     double pl = fma(y, lh, -ph);
     pl = fma(y, ll, pl);
     return sign * exp_ab(ph, pl);
+}
+
+/* (1/x)^y as exp(-y log x): no reciprocal on the dependency chain and no
+ * rounding of 1/x; positive finite x and finite nonzero y, anything else
+ * goes through pow(1/x, y) */
+__device__ __forceinline__ double pow_recip(double x, double y) {
+    if (!(x > 0.0 && x < 1.0e300 && x > 1.0e-300) || !(fabs(y) < 1.0e300) || y == 0.0) return pow(1.0 / x, y);
+    double lh, ll;
+    log_hl(x, lh, ll);
+    const double ny = -y;
+    double ph = ny * lh;
+    double pl = fma(ny, lh, -ph);
+    pl = fma(ny, ll, pl);
+    return exp_ab(ph, pl);
 }
 
 /* sin(pi x), cos(pi x) */

@@ -50,7 +50,7 @@ __forceinline__ __device__ void CoupledSystems_PerBlock_OdeFunction(
     Precision* CPT, Precision* CPF)
 {
     Precision rx1 = 1.0 / X[0];
-    Precision p = bes::math::pow(rx1, uPAR[10]);
+    Precision p = bes::math::pow_recip(X[0], uPAR[10]);   /* (1/X0)^(3 kappa), off the reciprocal's chain */
     Precision s1, c1;
     bes::math::sincospi(2.0 * T, s1, c1);
     Precision s2, c2;

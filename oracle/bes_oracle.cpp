@@ -55,7 +55,7 @@ const double PI = 3.14159265358979323846;
 inline void km_ode(double X0, double X1, double T, const double* u,
                    double* F0, double* F1, double* CPT, double* CPF) {
     double rx1 = 1.0 / X0;
-    double p = oracle_math::pow(rx1, u[10]);
+    double p = oracle_math::pow_recip(X0, u[10]);   /* (1/X0)^u10 */
     double s1, c1;
     oracle_math::sincospi(2.0 * T, &s1, &c1);
     double s2, c2;
@@ -588,6 +588,7 @@ int bes_oracle_solve(const bes_oracle_problem* p, int n_periods, int reset_at,
 }
 
 double bes_oracle_pow(double x, double y) { return oracle_math::pow(x, y); }
+double bes_oracle_pow_recip(double x, double y) { return oracle_math::pow_recip(x, y); }
 double bes_oracle_exp(double x) { return oracle_math::exp(x); }
 double bes_oracle_log(double x) { return oracle_math::log(x); }
 void bes_oracle_sincospi(double x, double* s, double* c) { oracle_math::sincospi(x, s, c); }

@@ -94,6 +94,7 @@ int bes_oracle_solve(const bes_oracle_problem* p, int n_periods, int reset_at,
 
 /* Elementary functions of the oracle (for the accuracy tests). */
 double bes_oracle_pow(double x, double y);
+double bes_oracle_pow_recip(double x, double y);   /* (1/x)^y */
 double bes_oracle_exp(double x);
 double bes_oracle_log(double x);
 void bes_oracle_sincospi(double x, double* s, double* c);

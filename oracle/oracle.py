@@ -62,8 +62,9 @@ def lib() -> ctypes.CDLL:
         for n in ("bes_oracle_exp", "bes_oracle_log"):
             getattr(L, n).argtypes = [ctypes.c_double]
             getattr(L, n).restype = ctypes.c_double
-        L.bes_oracle_pow.argtypes = [ctypes.c_double, ctypes.c_double]
-        L.bes_oracle_pow.restype = ctypes.c_double
+        for n in ("bes_oracle_pow", "bes_oracle_pow_recip"):
+            getattr(L, n).argtypes = [ctypes.c_double, ctypes.c_double]
+            getattr(L, n).restype = ctypes.c_double
         L.bes_oracle_sincospi.argtypes = [ctypes.c_double, _dp, _dp]
         L.bes_oracle_sincos.argtypes = [ctypes.c_double, _dp, _dp]
         L.bes_oracle_rhs.argtypes = [ctypes.c_int, ctypes.c_double, _dp, _dp, _dp, ctypes.c_int, _dp]

@@ -183,6 +183,19 @@ static inline double pow(double x, double y) {
     return sign * exp_ab(ph, pl);
 }
 
+/* (1/x)^y as exp(-y log x); positive finite x and finite nonzero y, anything
+ * else through pow(1/x, y) (device: bes_math.cuh pow_recip) */
+static inline double pow_recip(double x, double y) {
+    if (!(x > 0.0 && x < 1.0e300 && x > 1.0e-300) || !(std::fabs(y) < 1.0e300) || y == 0.0) return pow(1.0 / x, y);
+    double lh, ll;
+    log_hl(x, &lh, &ll);
+    const double ny = -y;
+    double ph = ny * lh;
+    double pl = std::fma(ny, lh, -ph);
+    pl = std::fma(ny, ll, pl);
+    return exp_ab(ph, pl);
+}
+
 /* sin(pi x), cos(pi x) */
 static inline void sincospi(double x, double* s, double* c) {
     if (!std::isfinite(x)) { *s = NAN; *c = NAN; return; }

@@ -44,6 +44,18 @@ def test_pow_faithful(oracle_lib):
     assert worst <= 1.0
 
 
+def test_pow_recip_faithful(oracle_lib):
+    """(1/x)^y as exp(-y log x), the Keller-Miksis gas-pressure term's form."""
+    L = oracle_lib.lib()
+    rng = np.random.default_rng(3)
+    worst = 0.0
+    for x in 10 ** rng.uniform(-2.5, 2.5, 400):
+        for y in (4.2, 3.0 * 1.4, 1.0, 0.3):
+            got = L.bes_oracle_pow_recip(float(x), y)
+            worst = max(worst, _ulp_err(got, (-(D(float(x)).ln() * D(y))).exp()))
+    assert worst <= 1.0
+
+
 def test_exp_log_faithful(oracle_lib):
     L = oracle_lib.lib()
     rng = np.random.default_rng(1)
