@@ -58,8 +58,10 @@ WORKLOADS = {
                    "f2 = k f1 (f1 U(20,100) kHz, k in {2,3}, amplitudes U(0,1.5) bar), rtol = atol alternating "
                    "1e-8 / 1e-10, one launch plan for all sizes; one step = one acoustic period of every system from rest"),
     "c3_period1": ("c3_period1: 4096 systems sharing one N = 128 cloud (1 mm cube, R_E lognormal median 4 um sigma 0.4 "
-                   "clipped to [1,12] um, seed 3), 200 kHz at 1.2 bar, initial radii perturbed by 1e-3 U(-1,1) per "
-                   "bubble, RKCK45 rtol=atol=1e-10, FP64 BiCG; one step = one acoustic period of every system from rest"),
+                   "clipped to [1,12] um, seed 3; the matrix R_j^3/(R_i^2 d_ij) given as the symmetric G = 1/d staged "
+                   "once per CTA with unit factors R^-2, R^3), 200 kHz at 1.2 bar, initial radii perturbed by 1e-3 "
+                   "U(-1,1) per bubble, RKCK45 rtol=atol=1e-10, FP64 BiCG; one step = one acoustic period of every "
+                   "system from rest"),
     "c3r_period1": ("c3r_period1: 4096 systems sharing one N = 128 geometry (1 mm cube, seed 3, G_ij = 1/d_ij staged "
                     "once per CTA), each system with its own radii (lognormal median 4 um sigma 0.4 clipped to "
                     "[1,12] um, seed 3+s) through the unit factors a_i = R_i^-2, b_j = R_j^3, 200 kHz at 1.2 bar, "

@@ -101,6 +101,7 @@ struct bes_solver {
     int class_begin[3] = {0, 0, 0}, class_count[3] = {0, 0, 0};
     bool class0_all32 = false;
     bool class_shared[3] = {false, false, false};   /* every system of the class uses one matrix */
+    bool class_symmetric[3] = {false, false, false}; /* ... and that matrix equals its transpose exactly */
     int sm_count = 148;
     /* the classes run concurrently: fork/join streams, and the whole solve is
      * captured once into a CUDA graph that later calls replay */
@@ -219,6 +220,7 @@ int units_class(int n) { return n <= 32 ? 0 : (n <= 64 ? 1 : 2); }
 bes_status copy_h2d(bes_solver* h, int id) {
     Buf& b = h->buf[id];
     if (b.count > 0) CUDA_TRY(h, cudaMemcpyAsync(b.d, b.h, b.bytes(), cudaMemcpyHostToDevice, h->stream));
+    if (id == B_COUPLING) h->order_dirty = true;   /* the shared-matrix kernels depend on the matrix's symmetry */
     if (id == B_CROW || id == B_CCOL) {
         const double* v = (const double*)b.h;
         bool any = false;
@@ -284,6 +286,17 @@ bes_status build_order(bes_solver* h) {
         for (int i = 1; i < h->class_count[c]; i++)
             if (h->matrix_of_system[idx[h->class_begin[c] + i]] != h->matrix_of_system[idx[h->class_begin[c]]])
                 h->class_shared[c] = false;
+        /* a symmetric shared matrix lets one shared-memory read serve both BiCG products */
+        h->class_symmetric[c] = false;
+        if (h->class_shared[c]) {
+            const int m = h->matrix_of_system[idx[h->class_begin[c]]];
+            const int n = h->matrix_dim[m];
+            const double* C = (const double*)h->buf[B_COUPLING].h + h->matrix_offset[m];
+            bool sym = true;
+            for (int i = 0; i < n && sym; i++)
+                for (int j = i + 1; j < n && sym; j++) sym = C[i + (int64_t)j * n] == C[j + (int64_t)i * n];
+            h->class_symmetric[c] = sym;
+        }
     }
     if (nact > 0)
         CUDA_TRY(h, cudaMemcpyAsync(h->d_order, h->h_order, sizeof(int32_t) * nact, cudaMemcpyHostToDevice, h->stream));
@@ -359,7 +372,7 @@ struct ClassLaunch {
 /* launch shape of one class (no stream work: safe before a capture) */
 bes_status plan_shape(bes_solver* h, int cls, int warps_per_system, int requested_wpb, ClassLaunch* L) {
     const bes::Variant v = bes::class_variant(cls, h->class0_all32, h->shared_coupling && h->class_shared[cls],
-                                         warps_per_system);
+                                         warps_per_system, h->class_symmetric[cls]);
     const int count = h->class_count[cls];
     if (bes::max_warps_per_block(v) < v.G)
         return fail(h, BES_ERR_CUDA, "solver kernel variant (U=%d, G=%d) does not fit in shared memory", v.U, v.G);
@@ -1039,7 +1052,7 @@ bes_status bes_solve_periods(bes_solver* h, int32_t n_periods, int32_t reset_at)
         if (h->class_count[cls] > 0 && (st = plan_class(h, cls, &L[cls]))) return st;
     if (h->scaled_coupling[0] || h->scaled_coupling[1])
         for (int cls = 0; cls < 3; cls++)
-            if (h->class_count[cls] > 0 && L[cls].v.rhs != 3)
+            if (h->class_count[cls] > 0 && L[cls].v.rhs != 3 && L[cls].v.rhs != 4)
                 return fail(h, BES_ERR_ARGUMENT,
                             "bes_solve_periods: CouplingRowScale / CouplingColumnScale hold values other than 1, "
                             "which only the shared-matrix kernels apply: turn SharedCouplingMatrices on and give "
@@ -1245,7 +1258,8 @@ bes_status bes_autotune(bes_solver* h, int32_t n_periods, int64_t step_cap, bes_
         int best_wps = 0, best_wpb = 0;
         for (int wps = 0; wps <= (cls == 0 ? 0 : 1) && !st; wps++) {
             const bes::Variant v = bes::class_variant(cls, h->class0_all32,
-                                                      h->shared_coupling && h->class_shared[cls], wps);
+                                                      h->shared_coupling && h->class_shared[cls], wps,
+                                                      h->class_symmetric[cls]);
             const int cap = bes::max_warps_per_block(v);
             for (int wpb = v.G; wpb <= cap && !st; wpb *= 2) {
                 ClassLaunch L;

@@ -630,7 +630,7 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
  * with G row sums as four interleaved fma chains and G column sums in the
  * halving-tree order over 32UG; the oracle's shared-matrix association
  * computes the same (a = b = 1 reproduces the unscaled products bit for bit). */
-template <int U, int G>
+template <int U, int G, bool SYM>
 __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const DeviceProblem& P, double T,
                                                    double (&Xs)[U][UD], double (&F)[U][UD],
                                                    double (&up)[U][NUPa], double (&ua)[U][NUAa],
@@ -692,9 +692,49 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const Dev
 #pragma unroll
         for (int m = 0; m < U; m++) out[m] = (a0[m] + a1[m]) + (a2[m] + a3[m]);
     };
+    /* the same row sums for two vectors at once: each matrix entry read from
+     * shared memory once (the kernel is bound by shared-memory reads), the
+     * chains and their order per vector as in row_sums */
+    auto row_sums2 = [&](const double2* v2, const double2* w2, double (&outv)[U], double (&outw)[U]) {
+        double a0[U], a1[U], a2[U], a3[U], b0[U], b1[U], b2[U], b3[U];
+#pragma unroll
+        for (int m = 0; m < U; m++) {
+            a0[m] = 0.0; a1[m] = 0.0; a2[m] = 0.0; a3[m] = 0.0;
+            b0[m] = 0.0; b1[m] = 0.0; b2[m] = 0.0; b3[m] = 0.0;
+        }
+#pragma unroll 2
+        for (int j = 0; j < NMAX; j += 4) {
+            const double2 va = v2[j / 2], vb = v2[j / 2 + 1];
+            const double2 wa = w2[j / 2], wb = w2[j / 2 + 1];
+#pragma unroll
+            for (int m = 0; m < U; m++) {
+                const double* Crow = S.W + S.unit(m);
+                if (j < N) { const double c = Crow[j * LDC]; a0[m] = fma(c, va.x, a0[m]); b0[m] = fma(c, wa.x, b0[m]); }
+                if (j + 1 < N) {
+                    const double c = Crow[(j + 1) * LDC];
+                    a1[m] = fma(c, va.y, a1[m]);
+                    b1[m] = fma(c, wa.y, b1[m]);
+                }
+                if (j + 2 < N) {
+                    const double c = Crow[(j + 2) * LDC];
+                    a2[m] = fma(c, vb.x, a2[m]);
+                    b2[m] = fma(c, wb.x, b2[m]);
+                }
+                if (j + 3 < N) {
+                    const double c = Crow[(j + 3) * LDC];
+                    a3[m] = fma(c, vb.y, a3[m]);
+                    b3[m] = fma(c, wb.y, b3[m]);
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < U; m++) {
+            outv[m] = (a0[m] + a1[m]) + (a2[m] + a3[m]);
+            outw[m] = (b0[m] + b1[m]) + (b2[m] + b3[m]);
+        }
+    };
     double bsum[U], asum[U];
-    row_sums(cpt2, bsum);
-    row_sums(z2, asum);
+    row_sums2(cpt2, z2, bsum, asum);
 #pragma unroll
     for (int m = 0; m < U; m++) {
         if (S.unit(m) < N) {
@@ -738,6 +778,10 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const Dev
         }
         grp_sync(S);
         double qs[U], qts[U];
+        if constexpr (SYM) {
+            /* C = C^T: the transposed product is a row sum too, from the same reads */
+            row_sums2(z2, zt2, qs, qts);
+        } else {
         row_sums(z2, qs);
 #pragma unroll
         for (int m = 0; m < U; m++) {
@@ -765,6 +809,7 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const Dev
             }
             auto leaf = [&](int k) -> double { return u[k]; };
             qts[m] = TreeSum<1, 32>::run(0, leaf);
+        }
         }
         double q[U], qt[U];
 #pragma unroll
@@ -806,8 +851,8 @@ __device__ __forceinline__ int rhs_eval(const Sys<U, G>& S, const DeviceProblem&
                                         bool& capped) {
     if constexpr (RHS == 0) {
         return coupled_rhs<U, G>(S, P, T, Xs, F, up, ua, iua, capped);
-    } else if constexpr (RHS == 3) {
-        return coupled_rhs_sharedc<U, G>(S, P, T, Xs, F, up, ua, iua, ra, cb, capped);
+    } else if constexpr (RHS == 3 || RHS == 4) {
+        return coupled_rhs_sharedc<U, G, RHS == 4>(S, P, T, Xs, F, up, ua, iua, ra, cb, capped);
     } else {
         static_assert(U == 1, "the register-resident operator needs one unit per lane");
         return coupled_rhs_regw<RHS == 2 ? 32 : 0>(S, P, T, Xs, F, up, ua, iua, capped);
@@ -1318,11 +1363,13 @@ __device__ __forceinline__ void analysis_period_end(const Sys<U, G>& S, const De
  * RHS = 0: operator W in shared memory; RHS = 1 / 2: operator in registers
  * (U = 1, G = 1; 2 = every system of the launch has exactly 32 units);
  * RHS = 3: every system of the launch shares one coupling matrix, staged once
- * per CTA (up to 8 warps per CTA).  G > 1 runs one unit per lane (U = 1) and
+ * per CTA (up to 8 warps per CTA), RHS = 4 the same for a symmetric matrix
+ * (both BiCG products as row sums from one read of each entry).  G > 1 runs
+ * one unit per lane (U = 1) and
  * exchanges the group's values through shared memory and a named barrier per
  * system slot (barrier 0 is left to __syncthreads). */
 template <int U, int RHS, int G>
-__global__ void __launch_bounds__(RHS == 3 || G > 1 ? 256 : 128, 1) bes_ensemble_kernel(DeviceProblem P) {
+__global__ void __launch_bounds__(RHS >= 3 || G > 1 ? 256 : 128, 1) bes_ensemble_kernel(DeviceProblem P) {
     static_assert(G == 1 || U == 1, "multi-warp systems run one unit per lane");
     static_assert(G == 1 || (RHS != 1 && RHS != 2), "the register-resident operator is single-warp");
     extern __shared__ double smem[];
@@ -1335,7 +1382,7 @@ __global__ void __launch_bounds__(RHS == 3 || G > 1 ? 256 : 128, 1) bes_ensemble
     S.bar = 1u + (unsigned)slot;
     S.xsel = 0;
     S.tot = P.total_units;
-    if constexpr (RHS == 3) {
+    if constexpr (RHS == 3 || RHS == 4) {
         /* one copy of the launch's shared coupling matrix per CTA, zero-padded */
         using SM = SharedCSmem<U, G>;
         constexpr int LDC = SM::LDC;
@@ -1410,7 +1457,7 @@ __global__ void __launch_bounds__(RHS == 3 || G > 1 ? 256 : 128, 1) bes_ensemble
 #pragma unroll
                 for (int c = 0; c < NUP; c++) L.up[m][c] = v ? __ldg(P.upar + (int64_t)c * S.tot + g) : 0.0;
             }
-            if constexpr (RHS == 3) {
+            if constexpr (RHS == 3 || RHS == 4) {
                 L.ra[m] = v ? (P.coupling_row_scale ? __ldg(P.coupling_row_scale + g) : 1.0) : 0.0;
                 L.cb[m] = v ? (P.coupling_col_scale ? __ldg(P.coupling_col_scale + g) : 1.0) : 0.0;
             } else {

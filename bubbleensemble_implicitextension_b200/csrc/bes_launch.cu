@@ -24,6 +24,10 @@ bool dispatch(Variant v, F&& f) {
         case 231: f(Tag<2, 3, 1>{}); return true;
         case 401: f(Tag<4, 0, 1>{}); return true;
         case 431: f(Tag<4, 3, 1>{}); return true;
+        case 241: f(Tag<2, 4, 1>{}); return true;
+        case 441: f(Tag<4, 4, 1>{}); return true;
+        case 142: f(Tag<1, 4, 2>{}); return true;
+        case 144: f(Tag<1, 4, 4>{}); return true;
         case 102: f(Tag<1, 0, 2>{}); return true;
         case 132: f(Tag<1, 3, 2>{}); return true;
         case 104: f(Tag<1, 0, 4>{}); return true;
@@ -46,7 +50,7 @@ size_t cta_smem_bytes(Variant v, int warps) {
 
 int max_warps_per_block(Variant v) {
     /* the kernels' launch bounds: 256 threads with RHS 3 or G > 1, else 128 */
-    const int cap = (v.rhs == 3 || v.G > 1) ? 8 : 4;
+    const int cap = (v.rhs >= 3 || v.G > 1) ? 8 : 4;
     int w = 0;
     while (w + v.G <= cap && cta_smem_bytes(v, w + v.G) <= 227 * 1024) w += v.G;
     return w;
@@ -69,9 +73,9 @@ cudaError_t launch(Variant v, const DeviceProblem& P, int grid, int warps, cudaS
  * on 2 or 4 warps (or 2 or 4 units per lane on one warp) with W in shared
  * memory, or one staged copy of a matrix shared by the whole class when the
  * caller asked for shared coupling matrices (SharedCouplingMatrices). */
-Variant class_variant(int cls, bool all32, bool shared, int warps_per_system) {
+Variant class_variant(int cls, bool all32, bool shared, int warps_per_system, bool symmetric) {
     if (cls == 0) return Variant{1, all32 ? 2 : 1, 1};
-    const int rhs = shared ? 3 : 0;
+    const int rhs = shared ? (symmetric ? 4 : 3) : 0;
     const int width = cls == 1 ? 2 : 4;
     if (warps_per_system == 1) return Variant{width, rhs, 1};
     return Variant{1, rhs, width};

@@ -6,7 +6,8 @@
  * N <= 64, 128).  RHS 0 keeps the operator in shared memory, RHS 1 keeps it
  * in registers (U = G = 1), RHS 2 is RHS 1 for launches whose systems all
  * have 32 units, RHS 3 stages one coupling matrix shared by the whole launch
- * per CTA (64 or 128 units). */
+ * per CTA (64 or 128 units), RHS 4 is RHS 3 for a symmetric shared matrix
+ * (both BiCG products as row sums from one shared-memory read). */
 #ifndef BES_LAUNCH_H
 #define BES_LAUNCH_H
 
@@ -36,7 +37,7 @@ cudaError_t launch(Variant v, const DeviceProblem& P, int grid, int warps, cudaS
 /* variant of units class cls (0: N <= 32, 1: N <= 64, 2: N <= 128); all32:
  * every system of the launch has 32 units; shared: the launch shares one
  * coupling matrix; warps_per_system 1 keeps every system on one warp */
-Variant class_variant(int cls, bool all32, bool shared, int warps_per_system);
+Variant class_variant(int cls, bool all32, bool shared, int warps_per_system, bool symmetric = false);
 /* warps per CTA for `count` systems of variant v (requested > 0: that many,
  * clamped to what the variant allows and rounded down to a multiple of G) */
 int class_warps_per_block(Variant v, int count, int sm_count, int requested);

@@ -322,15 +322,26 @@ def c2_ensemble(n_systems: int = 16384, seed: int = 2, n_periods: int = 64, rese
 
 def c3_ensemble(n_systems: int = 4096, n_units: int = 128, seed: int = 3, n_periods: int = 4, reset_at: int = -1,
                 cube_um: float = 1000.0, pa_bar: float = 1.2, f_khz: float = 200.0, rtol: float = 1e-10,
-                perturbation: float = 1e-3) -> Ensemble:
+                perturbation: float = 1e-3, factored: bool = True) -> Ensemble:
     """Shared-geometry ensemble: one N-bubble cloud (uniform in a cube, radii
     lognormal median 4 um, sigma 0.4, clipped to [1, 12] um) shared by every
     system; systems differ by a perturbed initial radius
-    y1(0) = 1 + perturbation * U(-1, 1) per bubble."""
+    y1(0) = 1 + perturbation * U(-1, 1) per bubble.
+
+    factored: the reference-format matrix C_ij = R_j^3 / (R_i^2 d_ij) given as
+    the symmetric geometry G_ij = 1/d_ij with the unit factors a_i = R_i^-2,
+    b_j = R_j^3 (the library then reads each entry of G once for both BiCG
+    products); otherwise C itself, as the reference stores it."""
     rng = np.random.default_rng(seed)
     pts = rng.uniform(0.0, cube_um, (n_units, 3))
     r = np.clip(np.exp(np.log(4.0) + 0.4 * rng.standard_normal(n_units)), 1.0, 12.0)
-    C = coupling_from_geometry(pts, r)
+    if factored:
+        d = np.sqrt(((pts[:, None, :] - pts[None, :, :]) ** 2).sum(-1))
+        off = ~np.eye(n_units, dtype=bool)
+        C = np.zeros((n_units, n_units))
+        C[off] = 1.0 / d[off]
+    else:
+        C = coupling_from_geometry(pts, r)
     up = km_unit_parameters(pa_bar, f_khz, 0.0, 0.0, 0.0, r)
     upar = np.tile(up, (1, n_systems))
     state = np.zeros((2, n_systems * n_units))
@@ -338,7 +349,9 @@ def c3_ensemble(n_systems: int = 4096, n_units: int = 128, seed: int = 3, n_peri
     return Ensemble(units=np.full(n_systems, n_units, dtype=np.int32), upar=upar, state=state,
                     coupling=C.T.reshape(-1).copy(), matrix_of_system=np.zeros(n_systems, dtype=np.int32),
                     rtol=np.full((2, n_systems), rtol), atol=np.full((2, n_systems), rtol), n_periods=n_periods,
-                    reset_at=reset_at, shared_matrices=True, name=f"c3_{n_systems}x{n_units}_shared")
+                    reset_at=reset_at, shared_matrices=True, name=f"c3_{n_systems}x{n_units}_shared",
+                    coupling_row_scale=np.tile(1.0 / (r * r), n_systems) if factored else None,
+                    coupling_col_scale=np.tile(r * r * r, n_systems) if factored else None)
 
 
 def c3_radii_ensemble(n_systems: int = 4096, n_units: int = 128, seed: int = 3, n_periods: int = 4,

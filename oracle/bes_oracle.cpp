@@ -135,7 +135,7 @@ struct Work {
 int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
                 const double* up, long ups, const double* C, int max_iter,
                 double* f0, double* f1, bool* capped, bool shared_assoc = false,
-                const double* ra = nullptr, const double* cb = nullptr) {
+                const double* ra = nullptr, const double* cb = nullptr, bool symmetric = false) {
     const int N = w.N;
     double upl[NUP];
     for (int i = 0; i < N; i++) {
@@ -195,8 +195,14 @@ int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
             if (shared_assoc) {
                 double s = row_sum4(N, [&](int j) { return C[i + (long)j * N]; }, [&](int j) { return w.b[j]; });
                 w.q[i] = fma(w.vs[i], s, w.p[i]);
-                for (int j = 0; j < N; j++) w.tmp2[j] = C[j + (long)i * N] * w.xu[j];
-                w.qt[i] = fma(w.us[i], tree_sum(w.tmp2.data(), N, w.tmp.data()), w.pt[i]);
+                if (symmetric) {
+                    /* C = C^T: the transposed product as a row sum (the kernel reads each entry once for both) */
+                    double st = row_sum4(N, [&](int j) { return C[i + (long)j * N]; }, [&](int j) { return w.xu[j]; });
+                    w.qt[i] = fma(w.us[i], st, w.pt[i]);
+                } else {
+                    for (int j = 0; j < N; j++) w.tmp2[j] = C[j + (long)i * N] * w.xu[j];
+                    w.qt[i] = fma(w.us[i], tree_sum(w.tmp2.data(), N, w.tmp.data()), w.pt[i]);
+                }
             } else {
                 w.q[i] = w.p[i] + row_sum4(N, [&](int j) { return w.W[i + (long)j * N]; }, [&](int j) { return w.p[j]; });
                 for (int j = 0; j < N; j++) w.tmp2[j] = w.W[j + (long)i * N] * w.pt[j];
@@ -255,13 +261,21 @@ struct SystemRun {
     }
     const double* up() const { return P->upar + off; }
     const double* C() const { return P->coupling + P->coupling_offset[s]; }
+    bool symmetric_C = false;   /* the system's matrix equals its transpose exactly */
+    void find_symmetry() {
+        const double* c = C();
+        bool sym = true;
+        for (int i = 0; i < N && sym; i++)
+            for (int j = i + 1; j < N && sym; j++) sym = c[i + (long)j * N] == c[j + (long)i * N];
+        symmetric_C = sym;
+    }
 
     int rhs(double T, const double* a0, const double* a1, double* f0, double* f1, int64_t& nbicg, bool& capped_any) {
         bool capped = false;
         int it = coupled_rhs(w, T, a0, a1, up(), tot, C(), P->bicg_max_iter, f0, f1, &capped,
                              P->shared_assoc != 0 && N > 32,
                              P->coupling_row_scale ? P->coupling_row_scale + off : nullptr,
-                             P->coupling_col_scale ? P->coupling_col_scale + off : nullptr);
+                             P->coupling_col_scale ? P->coupling_col_scale + off : nullptr, symmetric_C);
         nbicg += it;
         if (capped) capped_any = true;
         return it;
@@ -573,6 +587,7 @@ int bes_oracle_solve(const bes_oracle_problem* p, int n_periods, int reset_at,
 #endif
     for (int s = 0; s < nsys; s++) {
         SystemRun run(p, s);
+        run.find_symmetry();
         for (int per = 0; per < n_periods; per++) {
             if (per == reset_at) {
                 for (int i = 0; i < run.N; i++) {

@@ -81,14 +81,18 @@ def test_graph_replay_equals_direct_launches(gpu):
     assert_bitwise(replay, direct, KEYS)
 
 
-@pytest.mark.parametrize("n,seed,wps,wpb", [(128, 31, 0, 8), (100, 32, 1, 4), (64, 33, 0, 8), (48, 34, 1, 4),
-                                            (72, 35, 0, 4), (40, 36, 0, 2)])
-def test_shared_matrix_staged_per_cta(n, seed, wps, wpb, gpu, oracle_lib):
+@pytest.mark.parametrize("n,seed,wps,wpb,factored", [(128, 31, 0, 8, True), (100, 32, 1, 4, True),
+                                                     (64, 33, 0, 8, True), (48, 34, 1, 4, True), (72, 35, 0, 4, True),
+                                                     (40, 36, 0, 2, True), (128, 37, 0, 8, False),
+                                                     (100, 38, 1, 4, False), (64, 39, 0, 4, False)])
+def test_shared_matrix_staged_per_cta(n, seed, wps, wpb, factored, gpu, oracle_lib):
     """SharedCouplingMatrices on: one matrix for the whole launch, staged once per
     CTA; the products follow the oracle's shared-matrix association (on 2 or 4
-    warps per system, or one warp with 2 or 4 units per lane)."""
+    warps per system, or one warp with 2 or 4 units per lane).  factored: a
+    symmetric geometry with unit factors, both products as row sums from one
+    read; otherwise the reference-format (unsymmetric) matrix."""
     ens = bounded(W.c3_ensemble(n_systems=6, n_units=n, seed=seed, pa_bar=1.0, f_khz=150.0, n_periods=1,
-                                reset_at=-1, cube_um=400.0 * (n / 32) ** (1 / 3)))
+                                reset_at=-1, cube_um=400.0 * (n / 32) ** (1 / 3), factored=factored))
     got = run_gpu(ens, n_periods=1, reset_at=-1, shared_matrices=True, warps_per_block=wpb, warps_per_system=wps)
     want = oracle_lib.run(ens, n_periods=1, reset_at=-1, shared_assoc=True)
     assert_bitwise(got, want, KEYS)

@@ -21,7 +21,7 @@ def test_factored_matches_explicit_matrices():
 
 
 def test_unit_factors_reproduce_the_unscaled_association():
-    ens = W.c3_ensemble(n_systems=2, n_units=40, n_periods=1, cube_um=300.0)
+    ens = W.c3_ensemble(n_systems=2, n_units=40, n_periods=1, cube_um=300.0, factored=False)
     ens.max_steps_per_period = 50_000
     ones = dataclasses.replace(ens, coupling_row_scale=np.ones(ens.total_units),
                                coupling_col_scale=np.ones(ens.total_units))
@@ -29,3 +29,15 @@ def test_unit_factors_reproduce_the_unscaled_association():
     y = O.run(ones, n_periods=1, reset_at=-1)
     for k in ("state", "uacc", "iuacc", "n_accepted", "n_bicg_iter"):
         assert np.array_equal(x[k], y[k]), k
+
+
+def test_symmetric_and_general_shared_associations_agree():
+    """The same C3 systems given as the symmetric geometry with unit factors
+    (both products as row sums) and as the reference-format matrix (transposed
+    product as a column tree): equal physics, rounding-level differences."""
+    kw = dict(n_systems=2, n_units=48, n_periods=1, cube_um=350.0, seed=4)
+    a = O.run(W.c3_ensemble(factored=True, **kw), n_periods=1, reset_at=-1)
+    b = O.run(W.c3_ensemble(factored=False, **kw), n_periods=1, reset_at=-1)
+    rel = np.abs(a["state"] - b["state"]) / np.abs(b["state"])
+    assert rel.max() < 1e-6
+    assert np.array_equal(a["iuacc"], b["iuacc"])
