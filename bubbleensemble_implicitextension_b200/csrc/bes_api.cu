@@ -1052,7 +1052,7 @@ bes_status bes_solve_periods(bes_solver* h, int32_t n_periods, int32_t reset_at)
         if (h->class_count[cls] > 0 && (st = plan_class(h, cls, &L[cls]))) return st;
     if (h->scaled_coupling[0] || h->scaled_coupling[1])
         for (int cls = 0; cls < 3; cls++)
-            if (h->class_count[cls] > 0 && L[cls].v.rhs != 3 && L[cls].v.rhs != 4)
+            if (h->class_count[cls] > 0 && L[cls].v.rhs < 3)
                 return fail(h, BES_ERR_ARGUMENT,
                             "bes_solve_periods: CouplingRowScale / CouplingColumnScale hold values other than 1, "
                             "which only the shared-matrix kernels apply: turn SharedCouplingMatrices on and give "

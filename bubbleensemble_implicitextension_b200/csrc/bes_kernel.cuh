@@ -843,16 +843,122 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const Dev
     return done;
 }
 
+/* ---------------------------------------------------------------------------
+ * Coupled right-hand side for N <= 32 when the launch shares one symmetric
+ * matrix G (RHS = 5; 6 drops the N guards when every system has 32 units):
+ * lane i keeps row i of G in registers for the whole system -- nothing is
+ * formed per right-hand side -- and both BiCG products are row sums of that
+ * row against broadcast vectors, with the unit factors a, b as in
+ * coupled_rhs_sharedc<.., SYM = true> and the same arithmetic order. */
+template <int NFIX>
+__device__ __forceinline__ int coupled_rhs_regsym(const Sys<1>& S, const DeviceProblem& P, double T,
+                                                  double (&Xs)[1][UD], double (&F)[1][UD], double (&ua)[1][NUAa],
+                                                  int (&iua)[1][NIUAa], const double (&ra)[1], const double (&cb)[1],
+                                                  const double (&g)[32], bool& capped) {
+    const int N = NFIX ? NFIX : S.N;
+    const int i = S.lane;
+    const bool valid = i < N;
+    double xu = 0.0, rd = 0.0, x1 = 0.0;
+    __syncwarp();
+    if (valid) {
+        double Fl[UD], cpt, cpf;
+        CoupledSystems_PerBlock_OdeFunction<double>(S.sid, i, Fl, Xs[0], T, S.upsh + i * NUPa, S.sPAR, S.gPAR,
+                                                    S.igPAR, ua[0], iua[0], S.sACC, S.isACC, &cpt, &cpf);
+#pragma unroll
+        for (int k = 0; k < UD; k++) F[0][k] = Fl[k];
+        xu = Fl[IC];
+        rd = cpf * ra[0];                       /* v = rD a  */
+        x1 = cb[0] * (Xs[0][0] * Xs[0][0]);     /* u = b X1sq */
+        S.vcpt[i] = cb[0] * cpt;
+        S.vp[i] = x1 * xu;
+    } else {
+#pragma unroll
+        for (int k = 0; k < UD; k++) F[0][k] = 0.0;
+        S.vcpt[i] = 0.0;
+        S.vp[i] = 0.0;
+    }
+    __syncwarp();
+    /* row sums of G against two broadcast vectors, four interleaved chains each */
+    auto row_sums2 = [&](const double* v, const double* w, double& outv, double& outw) {
+        const double2* v2 = reinterpret_cast<const double2*>(v);
+        const double2* w2 = reinterpret_cast<const double2*>(w);
+        double a[4] = {0.0, 0.0, 0.0, 0.0}, b[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int j = 0; j < 32; j += 2) {
+            const double2 vv = v2[j / 2], ww = w2[j / 2];
+            if (NFIX != 0 || j < N) { a[j & 3] = fma(g[j], vv.x, a[j & 3]); b[j & 3] = fma(g[j], ww.x, b[j & 3]); }
+            if (NFIX != 0 || j + 1 < N) {
+                a[(j + 1) & 3] = fma(g[j + 1], vv.y, a[(j + 1) & 3]);
+                b[(j + 1) & 3] = fma(g[j + 1], ww.y, b[(j + 1) & 3]);
+            }
+        }
+        outv = (a[0] + a[1]) + (a[2] + a[3]);
+        outw = (b[0] + b[1]) + (b[2] + b[3]);
+    };
+    double bsum, asum;
+    row_sums2(S.vcpt, S.vp, bsum, asum);
+    double r = 0.0;
+    if (valid) {
+        const double b = fma(rd, bsum, xu);
+        const double ax = fma(rd, asum, xu);
+        r = b - ax;
+    }
+    double rt = r, x = xu, p = 0.0, pt = 0.0;
+    double prod[1] = {r * rt};
+    double rho1 = warp_tree_sum<1>(prod);
+    double rho2 = 0.0;
+    int done = 0;
+    bool exited = false;
+    for (int iter = 1; iter <= P.bicg_max_iter; iter++) {
+        if (iter == 1) {
+            p = r;
+            pt = rt;
+            if (fabs(rho1) < 1e-6) { exited = true; break; }
+        } else {
+            const double beta = rho1 / rho2;
+            p = fma(beta, p, r);
+            pt = fma(beta, pt, rt);
+        }
+        __syncwarp();
+        S.vp[i] = x1 * p;     /* z  = u p  */
+        S.vpt[i] = rd * pt;   /* z~ = v p~ */
+        __syncwarp();
+        double qs, qts;
+        row_sums2(S.vp, S.vpt, qs, qts);
+        const double q = valid ? fma(rd, qs, p) : 0.0;
+        const double qt = valid ? fma(x1, qts, pt) : 0.0;
+        prod[0] = pt * q;
+        const double alpha = rho1 / warp_tree_sum<1>(prod);
+        x = fma(alpha, p, x);
+        r = fma(-alpha, q, r);
+        rt = fma(-alpha, qt, rt);
+        double ar[1] = {fabs(r)};
+        prod[0] = r * rt;
+        double rho_next;
+        const bool small = grp_sum_max_below<1, 1>(S, ar, prod, 1e-6, rho_next);
+        rho2 = rho1;
+        done++;
+        if (small) { exited = true; break; }
+        rho1 = rho_next;
+    }
+    if (!exited) capped = true;
+    F[0][IC] = x;
+    return done;
+}
+
 /* the right-hand side a kernel variant uses */
 template <int U, int RHS, int G>
 __device__ __forceinline__ int rhs_eval(const Sys<U, G>& S, const DeviceProblem& P, double T, double (&Xs)[U][UD],
                                         double (&F)[U][UD], double (&up)[U][NUPa], double (&ua)[U][NUAa],
                                         int (&iua)[U][NIUAa], const double (&ra)[U], const double (&cb)[U],
-                                        bool& capped) {
+                                        const double (&grow)[32], bool& capped) {
     if constexpr (RHS == 0) {
         return coupled_rhs<U, G>(S, P, T, Xs, F, up, ua, iua, capped);
     } else if constexpr (RHS == 3 || RHS == 4) {
         return coupled_rhs_sharedc<U, G, RHS == 4>(S, P, T, Xs, F, up, ua, iua, ra, cb, capped);
+    } else if constexpr (RHS == 5 || RHS == 6) {
+        static_assert(U == 1 && G == 1, "the register-resident operator needs one unit per lane");
+        return coupled_rhs_regsym<RHS == 6 ? 32 : 0>(S, P, T, Xs, F, ua, iua, ra, cb, grow, capped);
     } else {
         static_assert(U == 1, "the register-resident operator needs one unit per lane");
         return coupled_rhs_regw<RHS == 2 ? 32 : 0>(S, P, T, Xs, F, up, ua, iua, capped);
@@ -868,6 +974,7 @@ struct Lane {
     int iua[U][NIUAa];
     double ev_a[U][NEa], ev_n[U][NEa];
     double ra[U], cb[U];   /* coupling factors a_i, b_i of the shared-matrix kernels */
+    double grow[32];       /* row of the shared symmetric matrix (RHS 5, 6) */
 };
 
 struct Counters {
@@ -937,7 +1044,7 @@ __device__ __forceinline__ bool step_rkck45(const Sys<U, G>& S, const DeviceProb
                     Xs[m][c] = fma(acc, dt, L.X[m][c]);
                 }
         }
-        cnt.bicg += rhs_eval<U, RHS, G>(S, P, Ts, Xs, F, L.up, L.ua, L.iua, L.ra, L.cb, capped);
+        cnt.bicg += rhs_eval<U, RHS, G>(S, P, Ts, Xs, F, L.up, L.ua, L.iua, L.ra, L.cb, L.grow, capped);
 #pragma unroll
         for (int j = 0; j < 6; j++)
 #pragma unroll
@@ -1004,7 +1111,7 @@ __device__ __forceinline__ bool step_rk4(const Sys<U, G>& S, const DeviceProblem
                     Xs[m][c] = st == 3 ? fma(kprev, dt, L.X[m][c]) : fma(kprev * kRK4_A[st], dt, L.X[m][c]);
                 }
         }
-        cnt.bicg += rhs_eval<U, RHS, G>(S, P, Ts, Xs, F, L.up, L.ua, L.iua, L.ra, L.cb, capped);
+        cnt.bicg += rhs_eval<U, RHS, G>(S, P, Ts, Xs, F, L.up, L.ua, L.iua, L.ra, L.cb, L.grow, capped);
 #pragma unroll
         for (int j = 0; j < 4; j++)
 #pragma unroll
@@ -1369,9 +1476,10 @@ __device__ __forceinline__ void analysis_period_end(const Sys<U, G>& S, const De
  * exchanges the group's values through shared memory and a named barrier per
  * system slot (barrier 0 is left to __syncthreads). */
 template <int U, int RHS, int G>
-__global__ void __launch_bounds__(RHS >= 3 || G > 1 ? 256 : 128, 1) bes_ensemble_kernel(DeviceProblem P) {
+__global__ void __launch_bounds__(RHS == 3 || RHS == 4 || G > 1 ? 256 : 128, 1) bes_ensemble_kernel(DeviceProblem P) {
     static_assert(G == 1 || U == 1, "multi-warp systems run one unit per lane");
-    static_assert(G == 1 || (RHS != 1 && RHS != 2), "the register-resident operator is single-warp");
+    static_assert(G == 1 || (RHS != 1 && RHS != 2 && RHS != 5 && RHS != 6),
+                  "the register-resident operators are single-warp");
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -1457,7 +1565,7 @@ __global__ void __launch_bounds__(RHS >= 3 || G > 1 ? 256 : 128, 1) bes_ensemble
 #pragma unroll
                 for (int c = 0; c < NUP; c++) L.up[m][c] = v ? __ldg(P.upar + (int64_t)c * S.tot + g) : 0.0;
             }
-            if constexpr (RHS == 3 || RHS == 4) {
+            if constexpr (RHS >= 3) {
                 L.ra[m] = v ? (P.coupling_row_scale ? __ldg(P.coupling_row_scale + g) : 1.0) : 0.0;
                 L.cb[m] = v ? (P.coupling_col_scale ? __ldg(P.coupling_col_scale + g) : 1.0) : 0.0;
             } else {
@@ -1473,6 +1581,12 @@ __global__ void __launch_bounds__(RHS >= 3 || G > 1 ? 256 : 128, 1) bes_ensemble
             for (int c = lane; c < NSP; c += 32) S.sPAR[c] = P.spar[(int64_t)c * P.n_systems + sid];
             for (int c = lane; c < NSA; c += 32) S.sACC[c] = P.sacc[(int64_t)c * P.n_systems + sid];
             for (int c = lane; c < NISA; c += 32) S.isACC[c] = P.isacc[(int64_t)c * P.n_systems + sid];
+        }
+        if constexpr (RHS == 5 || RHS == 6) {
+            /* row `lane` of the shared symmetric matrix, zero-padded to 32 */
+#pragma unroll
+            for (int j = 0; j < 32; j++)
+                L.grow[j] = (lane < S.N && j < S.N) ? __ldg(S.C + lane + (int64_t)j * S.N) : 0.0;
         }
         if constexpr (RHS == 1 || RHS == 2) {
             /* stage the system's coupling matrix, zero-padded to 32 x 33 */

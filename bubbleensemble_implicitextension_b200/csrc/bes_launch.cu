@@ -20,6 +20,8 @@ bool dispatch(Variant v, F&& f) {
     switch (key) {
         case 111: f(Tag<1, 1, 1>{}); return true;
         case 121: f(Tag<1, 2, 1>{}); return true;
+        case 151: f(Tag<1, 5, 1>{}); return true;
+        case 161: f(Tag<1, 6, 1>{}); return true;
         case 201: f(Tag<2, 0, 1>{}); return true;
         case 231: f(Tag<2, 3, 1>{}); return true;
         case 401: f(Tag<4, 0, 1>{}); return true;
@@ -50,7 +52,7 @@ size_t cta_smem_bytes(Variant v, int warps) {
 
 int max_warps_per_block(Variant v) {
     /* the kernels' launch bounds: 256 threads with RHS 3 or G > 1, else 128 */
-    const int cap = (v.rhs >= 3 || v.G > 1) ? 8 : 4;
+    const int cap = (v.rhs == 3 || v.rhs == 4 || v.G > 1) ? 8 : 4;
     int w = 0;
     while (w + v.G <= cap && cta_smem_bytes(v, w + v.G) <= 227 * 1024) w += v.G;
     return w;
@@ -74,7 +76,10 @@ cudaError_t launch(Variant v, const DeviceProblem& P, int grid, int warps, cudaS
  * memory, or one staged copy of a matrix shared by the whole class when the
  * caller asked for shared coupling matrices (SharedCouplingMatrices). */
 Variant class_variant(int cls, bool all32, bool shared, int warps_per_system, bool symmetric) {
-    if (cls == 0) return Variant{1, all32 ? 2 : 1, 1};
+    if (cls == 0) {
+        if (shared && symmetric) return Variant{1, all32 ? 6 : 5, 1};   /* row of G in registers */
+        return Variant{1, all32 ? 2 : 1, 1};
+    }
     const int rhs = shared ? (symmetric ? 4 : 3) : 0;
     const int width = cls == 1 ? 2 : 4;
     if (warps_per_system == 1) return Variant{width, rhs, 1};

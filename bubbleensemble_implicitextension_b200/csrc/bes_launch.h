@@ -7,7 +7,9 @@
  * in registers (U = G = 1), RHS 2 is RHS 1 for launches whose systems all
  * have 32 units, RHS 3 stages one coupling matrix shared by the whole launch
  * per CTA (64 or 128 units), RHS 4 is RHS 3 for a symmetric shared matrix
- * (both BiCG products as row sums from one shared-memory read). */
+ * (both BiCG products as row sums from one shared-memory read); RHS 5 / 6
+ * (U = G = 1, N <= 32) keep a row of a shared symmetric matrix in registers
+ * (6: every system has 32 units). */
 #ifndef BES_LAUNCH_H
 #define BES_LAUNCH_H
 

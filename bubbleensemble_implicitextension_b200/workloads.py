@@ -237,16 +237,28 @@ class Ensemble:
 
 def c1_ensemble(n_pa: int = 16, n_f: int = 16, n_units: int = 32, spacing_um: float = 150.0,
                 seed: int = 1, rtol: float = 1e-10, atol: float = 1e-10, n_periods: int = 64,
-                reset_at: int = 32, cstr: float = 1.0, pa_range=(0.5, 2.0), f_range=(20.0, 200.0)) -> Ensemble:
+                reset_at: int = 32, cstr: float = 1.0, pa_range=(0.5, 2.0), f_range=(20.0, 200.0),
+                factored: bool = False) -> Ensemble:
     """Plain-method small ensemble: n_pa x n_f systems of N bubbles on a 1-D line.
 
     Amplitude linspace over pa_range (bar), frequency logspace over f_range
     (kHz), frequency outer and amplitude inner as in CollapseStrength.cu:306-308;
-    equilibrium radii U(2, 8) um from PCG64(seed), bubble i at x = spacing * i."""
+    equilibrium radii U(2, 8) um from PCG64(seed), bubble i at x = spacing * i.
+
+    factored: the reference-format matrix cstr R_j^3 / (R_i^2 d_ij) given as the
+    symmetric geometry G_ij = cstr / d_ij shared by the launch with the unit
+    factors a_i = R_i^-2, b_j = R_j^3 (SharedCouplingMatrices on), which keeps a
+    row of G in registers; otherwise the reference's own matrix."""
     rng = np.random.default_rng(seed)
     radii = rng.uniform(2.0, 8.0, n_units)
     pos = spacing_um * np.arange(n_units, dtype=np.float64)
-    C = coupling_from_geometry(pos, radii, cstr)
+    if factored:
+        d = np.abs(pos[:, None] - pos[None, :])
+        off = ~np.eye(n_units, dtype=bool)
+        C = np.zeros((n_units, n_units))
+        C[off] = cstr / d[off]
+    else:
+        C = coupling_from_geometry(pos, radii, cstr)
     pa = linspace_ref(pa_range[0], pa_range[1], n_pa)
     fr = logspace_ref(f_range[0], f_range[1], n_f)
     ns = n_pa * n_f
@@ -260,7 +272,10 @@ def c1_ensemble(n_pa: int = 16, n_f: int = 16, n_units: int = 32, spacing_um: fl
                     coupling=C.T.reshape(-1).copy(), matrix_of_system=np.zeros(ns, dtype=np.int32),
                     rtol=np.full((2, ns), rtol), atol=np.full((2, ns), atol), n_periods=n_periods, reset_at=reset_at,
                     name=f"c1_{ns}x{n_units}", info={"pa_bar": sys_pa, "f_khz": sys_f, "radii_um": radii,
-                                                     "positions_um": pos, "cstr": cstr})
+                                                     "positions_um": pos, "cstr": cstr},
+                    shared_matrices=factored,
+                    coupling_row_scale=np.tile(1.0 / (radii * radii), ns) if factored else None,
+                    coupling_col_scale=np.tile(radii ** 3, ns) if factored else None)
 
 
 def _ball_points(rng, count: int, radius: float) -> np.ndarray:

@@ -273,7 +273,7 @@ struct SystemRun {
     int rhs(double T, const double* a0, const double* a1, double* f0, double* f1, int64_t& nbicg, bool& capped_any) {
         bool capped = false;
         int it = coupled_rhs(w, T, a0, a1, up(), tot, C(), P->bicg_max_iter, f0, f1, &capped,
-                             P->shared_assoc != 0 && N > 32,
+                             P->shared_assoc != 0 && (N > 32 || symmetric_C),
                              P->coupling_row_scale ? P->coupling_row_scale + off : nullptr,
                              P->coupling_col_scale ? P->coupling_col_scale + off : nullptr, symmetric_C);
         nbicg += it;

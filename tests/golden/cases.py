@@ -25,13 +25,16 @@ RUNS = {
 }
 
 
-def build(name: str):
+def build(name: str, factored: bool = False):
+    """The case's ensemble with the reference-format coupling matrix (what the
+    reference harness ran), or, factored, the same physics as a shared
+    symmetric geometry with unit factors (the library's one-read kernels)."""
     spec, run = CASES[name], RUNS[name]
     if spec["kind"] == "c1":
-        ens = W.c1_ensemble().subset(spec["systems"])
+        ens = W.c1_ensemble(factored=factored).subset(spec["systems"])
     else:
         ens = W.c3_ensemble(n_systems=spec["n_systems"], n_units=spec["units"], seed=spec["seed"],
                             pa_bar=spec["pa_bar"], f_khz=spec["f_khz"], cube_um=400.0 * (spec["units"] / 32) ** (1 / 3),
-                            n_periods=run["n_periods"], reset_at=run["reset_at"])
+                            n_periods=run["n_periods"], reset_at=run["reset_at"], factored=factored)
     ens.n_periods, ens.reset_at = run["n_periods"], run["reset_at"]
     return ens, run

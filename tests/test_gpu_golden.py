@@ -14,3 +14,13 @@ def test_kernel_matches_reference_golden(name, gpu):
     got = run_gpu(ens, n_periods=run["n_periods"], reset_at=run["reset_at"], ndo=run.get("ndo", 0),
                   do_min_dt=run.get("do_min_dt", 0.0), do_save_frequency=run.get("do_save_frequency", 1))
     golden_compare.check(name, got)
+
+
+@pytest.mark.parametrize("name", ["c1_n32", "cloud_n64", "cloud_n128"])
+def test_symmetric_geometry_kernels_match_reference_golden(name, gpu):
+    """The same systems as a shared symmetric geometry with unit factors (row of
+    G in registers for N = 32, one shared-memory read for both products above)
+    against the reference's own solver run on the reference-format matrix."""
+    ens, run = cases.build(name, factored=True)
+    got = run_gpu(ens, n_periods=run["n_periods"], reset_at=run["reset_at"])
+    golden_compare.check(name, got)

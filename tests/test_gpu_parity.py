@@ -162,3 +162,22 @@ def test_autotuned_shapes_give_identical_results(gpu):
     a = run_gpu(ens, n_periods=1, reset_at=-1)
     b = run_gpu(ens, n_periods=1, reset_at=-1, autotune=True)
     assert_bitwise(b, a, KEYS)
+
+
+def test_shared_symmetric_geometry_n32_row_in_registers(gpu, oracle_lib):
+    """C1 given as the shared symmetric line geometry with unit factors: the
+    N <= 32 kernel keeps a row of G in registers (RHS 6, and RHS 5 with ragged
+    sizes below), bit-identical to the oracle's shared association."""
+    ens = bounded(W.c1_ensemble(factored=True).subset([0, 3, 7, 64, 100, 128, 200, 250]))
+    got = run_gpu(ens, n_periods=2, reset_at=1)
+    want = oracle_lib.run(ens, n_periods=2, reset_at=1)
+    assert_bitwise(got, want, KEYS)
+    assert (got["iuacc"] >= 0).any()
+
+
+def test_shared_symmetric_geometry_ragged_n_le_32(gpu, oracle_lib):
+    full = W.c1_ensemble(factored=True, n_units=24, n_pa=4, n_f=2)
+    ens = bounded(full)
+    got = run_gpu(ens, n_periods=1, reset_at=-1)
+    want = oracle_lib.run(ens, n_periods=1, reset_at=-1)
+    assert_bitwise(got, want, KEYS)

@@ -41,3 +41,14 @@ def test_symmetric_and_general_shared_associations_agree():
     rel = np.abs(a["state"] - b["state"]) / np.abs(b["state"])
     assert rel.max() < 1e-6
     assert np.array_equal(a["iuacc"], b["iuacc"])
+
+
+def test_factored_line_matches_reference_format():
+    """C1 as the symmetric line geometry with unit factors (shared association)
+    against the reference-format matrix: one period, 1e-6 and equal events."""
+    kw = dict(n_pa=2, n_f=2, n_periods=1, reset_at=-1)
+    a = O.run(W.c1_ensemble(factored=True, **kw).subset([1, 2]), n_periods=1, reset_at=-1)
+    b = O.run(W.c1_ensemble(factored=False, **kw).subset([1, 2]), n_periods=1, reset_at=-1)
+    rel = np.abs(a["state"] - b["state"]) / np.abs(b["state"])
+    assert rel.max() < 1e-6
+    assert np.array_equal(a["iuacc"], b["iuacc"])
