@@ -46,7 +46,8 @@ sys.path.insert(0, str(ROOT))
 METRIC = "system-periods/sec at rtol 1e-10"
 UNIT = "system-periods/s"
 WORKLOAD = ("c1_period1: 256 systems (16 amplitudes 0.5-2 bar x 16 frequencies 20-200 kHz log) x 32 coupled "
-            "Keller-Miksis bubbles on a 1-D line (d = 150 um, R_E ~ U(2,8) um seed 1), RKCK45 rtol=atol=1e-10, "
+            "Keller-Miksis bubbles on a 1-D line (d = 150 um, R_E ~ U(2,8) um seed 1; coupling R_j^3/(R_i^2 d_ij) "
+            "given as the shared geometry 1/d_ij with unit factors unless --c1-format reference), RKCK45 rtol=atol=1e-10, "
             "dt0=1e-3, dtmin=1e-13, events dR/dt=0 (dir -1, tol 1e-4) with collapse recording; one step = one "
             "acoustic period of every system from rest")
 DATA = "synthetic: seeded PCG64 radii, reference parameter formulas (CollapseStrength.cu:329-357)"
@@ -74,10 +75,13 @@ WORKLOADS = {
 }
 
 
+args_c1_factored = True
+
+
 def make_ensemble(name):
     from bubbleensemble_implicitextension_b200 import workloads as W
     if name == "c1_period1":
-        return W.c1_ensemble(n_periods=1, reset_at=-1)
+        return W.c1_ensemble(n_periods=1, reset_at=-1, factored=args_c1_factored)
     if name == "c2_period1":
         return W.c2_ensemble(n_periods=1, reset_at=-1)
     if name == "c3r_period1":
@@ -106,6 +110,10 @@ def parse():
     ap.add_argument("--ref-regcap", choices=["capped", "uncapped"], default="uncapped",
                     help="reference arm: the reference built without its shipped -maxrregcount=128 (the faster of "
                          "the two on the B200: 44.8 vs 30.0 system-periods/s on c1_period1) or with it")
+    ap.add_argument("--c1-format", choices=["geometry", "reference"], default="geometry",
+                    help="c1_period1 coupling input: the symmetric line geometry 1/d shared by the launch with unit "
+                         "factors R^-2, R^3 (default; the same matrix R_j^3/(R_i^2 d_ij) as a product) or the "
+                         "reference-format matrix itself")
     ap.add_argument("--autotune", type=int, default=1, choices=[0, 1],
                     help="1: pick launch shapes with bes_autotune before the warm-up (untimed)")
     ap.add_argument("--warps-per-system", type=int, default=0, choices=[0, 1],
@@ -233,6 +241,8 @@ def run_b200(args, rank, world, local):
     V = S.ListOfVariables
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    global args_c1_factored
+    args_c1_factored = args.c1_format == "geometry"
     ens = make_ensemble(args.workload)
     if 0 < args.systems < ens.n_systems:
         ens = ens.subset(list(range(0, ens.n_systems, ens.n_systems // args.systems))[:args.systems])
@@ -336,6 +346,8 @@ def run_b200(args, rank, world, local):
                    "units_per_system": int(ens.units[0]) if len(set(ens.units.tolist())) == 1 else "mixed",
                    "total_units": ens.total_units,
                    "periods_per_step": 1,
+                   "coupling_input": ("shared symmetric geometry G = 1/d with unit factors R^-2, R^3"
+                                      if ens.coupling_row_scale is not None else "per-ensemble matrix as given"),
                    "warps_per_system": "one" if args.warps_per_system else "2 or 4 above 32 units",
                    "launch_shapes": tuned if tuned else "heuristic",
                    "l2": "flushed between timed steps (256 MiB write, untimed)",
