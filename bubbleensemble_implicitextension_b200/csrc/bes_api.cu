@@ -72,6 +72,7 @@ struct bes_solver {
     int64_t total_units = 0;
     int n_matrices = 1;
     std::vector<int32_t> matrix_of_system, matrix_dim;
+    std::vector<char> matrix_symmetric;   /* per matrix, as last copied to the device (exact C == C^T) */
     std::vector<int64_t> matrix_offset, coupling_offset;
     Buf buf[B_COUNT];
     /* device-only metadata */
@@ -220,7 +221,20 @@ int units_class(int n) { return n <= 32 ? 0 : (n <= 64 ? 1 : 2); }
 bes_status copy_h2d(bes_solver* h, int id) {
     Buf& b = h->buf[id];
     if (b.count > 0) CUDA_TRY(h, cudaMemcpyAsync(b.d, b.h, b.bytes(), cudaMemcpyHostToDevice, h->stream));
-    if (id == B_COUPLING) h->order_dirty = true;   /* the shared-matrix kernels depend on the matrix's symmetry */
+    if (id == B_COUPLING) {
+        /* the shared-matrix kernels depend on the symmetry of what the device holds */
+        const double* C = (const double*)b.h;
+        h->matrix_symmetric.assign(h->n_matrices, 0);
+        for (int m = 0; m < h->n_matrices; m++) {
+            const int n = h->matrix_dim[m];
+            const double* Cm = C + h->matrix_offset[m];
+            bool sym = true;
+            for (int i = 0; i < n && sym; i++)
+                for (int j = i + 1; j < n && sym; j++) sym = Cm[i + (int64_t)j * n] == Cm[j + (int64_t)i * n];
+            h->matrix_symmetric[m] = sym;
+        }
+        h->order_dirty = true;
+    }
     if (id == B_CROW || id == B_CCOL) {
         const double* v = (const double*)b.h;
         bool any = false;
@@ -290,12 +304,7 @@ bes_status build_order(bes_solver* h) {
         h->class_symmetric[c] = false;
         if (h->class_shared[c]) {
             const int m = h->matrix_of_system[idx[h->class_begin[c]]];
-            const int n = h->matrix_dim[m];
-            const double* C = (const double*)h->buf[B_COUPLING].h + h->matrix_offset[m];
-            bool sym = true;
-            for (int i = 0; i < n && sym; i++)
-                for (int j = i + 1; j < n && sym; j++) sym = C[i + (int64_t)j * n] == C[j + (int64_t)i * n];
-            h->class_symmetric[c] = sym;
+            h->class_symmetric[c] = m < (int)h->matrix_symmetric.size() && h->matrix_symmetric[m];
         }
     }
     if (nact > 0)
