@@ -1146,6 +1146,126 @@ bes_status bes_set_period_analysis(bes_solver* h, int32_t sections, double dista
     return BES_OK;
 }
 
+/* Print(var) / Print(var, n) of the reference (Interface.cuh:1809-1947 with
+ * its writers :1530-1805): the host mirror of a variable to
+ * <Name>InSolverObject.txt (CouplingMatrix: ..._<n>.txt; DenseOutput:
+ * DenseOutput_<system>.txt with the system's parameters, accessories and time
+ * series), every value in width 18, scientific with 10 digits, followed by a
+ * comma.  The unit-scope files have one row per unit (no thread padding
+ * rows: the library stores none). */
+bes_status bes_print(bes_solver* h, int32_t var, int32_t serial, const char* directory) {
+    bes_status st = check_solver(h);
+    if (st) return st;
+    const std::string dir = directory && directory[0] ? std::string(directory) + "/" : std::string();
+    const int W = 18;
+    auto open = [&](const std::string& name, std::ofstream& f) -> bool {
+        f.open(dir + name);
+        f.precision(10);
+        f.flags(std::ios::scientific);
+        return (bool)f;
+    };
+    auto value = [&](std::ofstream& f, int id, int64_t k) {
+        f.width(W);
+        if (is_int_buf(id)) f << ((const int32_t*)h->buf[id].h)[k];
+        else f << ((const double*)h->buf[id].h)[k];
+    };
+    const int64_t NS = h->n_systems, TU = h->total_units;
+    if (var == BES_COUPLING_MATRIX) {
+        if ((st = bound(h, "Print", "CouplingMatrix", serial, 0, (long long)h->n_matrices * h->nc - 1))) return st;
+        const int m = serial / h->nc, cn = serial % h->nc, n = h->matrix_dim[m];
+        std::ofstream f;
+        if (!open("CouplingMatrixInSolverObject_" + std::to_string(serial) + ".txt", f))
+            return fail(h, BES_ERR_IO, "Print: cannot open the coupling matrix file in '%s'", dir.c_str());
+        const int64_t base = h->matrix_offset[m] + (int64_t)cn * n * n;
+        for (int i = 0; i < n; i++) {
+            for (int j = 0; j < n; j++) { value(f, B_COUPLING, base + i + (int64_t)j * n); f << ','; }
+            f << '\n';
+        }
+        return f ? BES_OK : fail(h, BES_ERR_IO, "Print: writing the coupling matrix failed");
+    }
+    if (var == BES_DENSE_OUTPUT) {
+        if ((st = bound(h, "Print", "DenseOutput", serial, 0, NS - 1))) return st;
+        std::ofstream f;
+        if (!open("DenseOutput_" + std::to_string(serial) + ".txt", f))
+            return fail(h, BES_ERR_IO, "Print: cannot open the dense output file in '%s'", dir.c_str());
+        const int n = h->units[serial];
+        const int64_t off = h->unit_offset[serial];
+        auto unit_block = [&](const char* title, int id, int count) {
+            f << title << ":\n";
+            f.width(W); f << "Serial No." << ',';
+            for (int u = 0; u < n; u++) { f.width(W); f << "U" + std::to_string(u); if (u < n - 1) f << ','; }
+            f << '\n';
+            for (int k = 0; k < count; k++) {
+                f.width(W); f << k << ',';
+                for (int u = 0; u < n; u++) { value(f, id, (int64_t)k * TU + off + u); if (u < n - 1) f << ','; }
+                f << '\n';
+            }
+            f << '\n';
+        };
+        auto row_block = [&](const char* title, int id, int count, int64_t stride, int64_t first) {
+            f << title << ":\n";
+            for (int k = 0; k < count; k++) { value(f, id, first + (int64_t)k * stride); if (k < count - 1) f << ','; }
+            f << '\n' << '\n';
+        };
+        unit_block("UnitParameters", B_UPAR, h->nup);
+        unit_block("UnitAccessories", B_UACC, h->nua);
+        unit_block("IntegerUnitAccessories", B_IUACC, h->niua);
+        row_block("SystemParameters", B_SPAR, h->nsp, NS, serial);
+        row_block("SystemAccessories", B_SACC, h->nsa, NS, serial);
+        row_block("IntegerSystemAccessories", B_ISACC, h->nisa, NS, serial);
+        row_block("GlobalParameters", B_GPAR, h->ngp, 1, 0);
+        row_block("IntegerGlobalParameters", B_IGPAR, h->nigp, 1, 0);
+        f << "Time series:\n";
+        f.width(W); f << "t" << ',';
+        for (int u = 0; u < n; u++)
+            for (int c = 0; c < h->ud; c++) {
+                f.width(W); f << "U" + std::to_string(u) + "/C" + std::to_string(c);
+                if (u < n - 1 || c < h->ud - 1) f << ',';
+            }
+        f << '\n';
+        const int rows = h->ndo > 0 ? std::min(((const int32_t*)h->buf[B_DENSE_INDEX].h)[serial], h->ndo) : 0;
+        for (int i = 0; i < rows; i++) {
+            value(f, B_DENSE_TIME, (int64_t)i * NS + serial);
+            f << ',';
+            for (int u = 0; u < n; u++)
+                for (int c = 0; c < h->ud; c++) {
+                    value(f, B_DENSE_STATE, (int64_t)i * h->ud * TU + (int64_t)c * TU + off + u);
+                    if (u < n - 1 || c < h->ud - 1) f << ',';
+                }
+            f << '\n';
+        }
+        return f ? BES_OK : fail(h, BES_ERR_IO, "Print: writing the dense output failed");
+    }
+    int id = -1;
+    int64_t rows = 0, cols = 0;
+    switch (var) {
+        case BES_TIME_DOMAIN: id = B_TIME_DOMAIN; rows = NS; cols = 2; break;
+        case BES_ACTUAL_TIME: id = B_ACTUAL_TIME; rows = NS; cols = 1; break;
+        case BES_ACTUAL_STATE: id = B_STATE; rows = TU; cols = h->ud; break;
+        case BES_UNIT_PARAMETERS: id = B_UPAR; rows = TU; cols = h->nup; break;
+        case BES_SYSTEM_PARAMETERS: id = B_SPAR; rows = NS; cols = h->nsp; break;
+        case BES_GLOBAL_PARAMETERS: id = B_GPAR; rows = h->ngp; cols = 1; break;
+        case BES_INTEGER_GLOBAL_PARAMETERS: id = B_IGPAR; rows = h->nigp; cols = 1; break;
+        case BES_UNIT_ACCESSORIES: id = B_UACC; rows = TU; cols = h->nua; break;
+        case BES_INTEGER_UNIT_ACCESSORIES: id = B_IUACC; rows = TU; cols = h->niua; break;
+        case BES_SYSTEM_ACCESSORIES: id = B_SACC; rows = NS; cols = h->nsa; break;
+        case BES_INTEGER_SYSTEM_ACCESSORIES: id = B_ISACC; rows = NS; cols = h->nisa; break;
+        case BES_COUPLING_STRENGTH: id = B_COUPLING_STRENGTH; rows = NS; cols = h->nc; break;
+        case BES_COUPLING_INDEX: id = B_COUPLING_INDEX; rows = h->nc; cols = 1; break;
+        default:
+            return fail(h, BES_ERR_OPTION, "Print: option %s needs a different argument list or is not applicable",
+                        var_name(var));
+    }
+    std::ofstream f;
+    if (!open(std::string(var_name(var)) + "InSolverObject.txt", f))
+        return fail(h, BES_ERR_IO, "Print: cannot open the file for %s in '%s'", var_name(var), dir.c_str());
+    for (int64_t i = 0; i < rows; i++) {
+        for (int64_t j = 0; j < cols; j++) { value(f, id, i + j * rows); f << ','; }
+        f << '\n';
+    }
+    return f ? BES_OK : fail(h, BES_ERR_IO, "Print: writing %s failed", var_name(var));
+}
+
 /* The reference drivers' output files, written from the host mirrors (call
  * bes_synchronise_device_to_host for the variables first):
  *   BES_CSV_COLLAPSE   CollapseStrength.cu:174-198  (per system and record slot: id, uPAR15, uPAR16,

@@ -193,6 +193,7 @@ SIGNATURES = {
     "bes_autotune": [_P, _I32, ctypes.c_int64, ctypes.POINTER(AutotuneResult)],
     "bes_set_period_analysis": [_P, _I32, _D, _I32],
     "bes_write_csv": [_P, _I32, ctypes.c_char_p],
+    "bes_print": [_P, _I32, _I32, ctypes.c_char_p],
     "bes_create": [ctypes.POINTER(_Config), ctypes.POINTER(ctypes.c_void_p)],
     "bes_destroy": [_P],
     "bes_model_info_get": [ctypes.POINTER(ModelInfo)],
@@ -513,6 +514,11 @@ class ProblemSolver:
         """Per-period analysis of the following solves on the device (bes_set_period_analysis);
         sections < 0 turns it off."""
         self._ok(self._lib.bes_set_period_analysis(self._h, sections, distance_tolerance, accessory_index))
+
+    def Print(self, var: int, serial: int = 0, directory=None) -> None:
+        """Print(var) / Print(var, n) of the reference (bes_print): the host mirror to a text file."""
+        d = None if directory is None else str(directory).encode()
+        self._ok(self._lib.bes_print(self._h, var, serial, d))
 
     def write_csv(self, kind: int, path) -> None:
         """One of the reference drivers' output files from the host mirrors (bes_write_csv)."""

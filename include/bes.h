@@ -281,6 +281,12 @@ bes_status bes_measure_fp64_peak(int32_t device, double* tflops);
  * and accessory 0.  sections < 0 turns it off and frees the arrays. */
 bes_status bes_set_period_analysis(bes_solver* h, int32_t sections, double distance_tolerance,
                                    int32_t accessory_index);
+/* Print(var) and Print(var, n) of ProblemSolver (Interface.cuh:1809-1947):
+ * the host mirror of `var` to <Name>InSolverObject.txt in `directory` (NULL:
+ * the working directory) in the reference's layout and number format;
+ * serial selects the matrix (BES_COUPLING_MATRIX) or the system
+ * (BES_DENSE_OUTPUT: DenseOutput_<serial>.txt) and is ignored otherwise. */
+bes_status bes_print(bes_solver* h, int32_t var, int32_t serial, const char* directory);
 /* Output files of the reference drivers (CollapseStrength.cu:174-198,
  * BubbleEnsemble.cu:435-491) from the host mirrors, same layout and number
  * formats; kind is one of BES_CSV_*. */

@@ -217,33 +217,12 @@ class ProblemSolver {
         return (T)v;
     }
 
-    /* Print(ListOfVariables), Interface.cuh:1809-1914: the variable as CSV,
-     * one row per system (system scope) or unit (unit scope), to
-     * <Variable>InSolverObject.txt */
-    void Print(ListOfVariables Variable) {
-        int64_t n = 0;
-        bes_shim::check(bes_array_size(h_, Variable, &n), h_, "Print");
-        const bool is_int = Variable == IntegerGlobalParameters || Variable == IntegerUnitAccessories ||
-                            Variable == IntegerSystemAccessories || Variable == CouplingIndex || Variable == DenseIndex ||
-                            Variable == (ListOfVariables)BES_PERIOD_NUMBER;
-        std::vector<double> d;
-        std::vector<int32_t> iv;
-        if (is_int) { iv.resize(n); bes_shim::check(bes_get_array(h_, Variable, iv.data(), n), h_, "Print"); }
-        else { d.resize(n); bes_shim::check(bes_get_array(h_, Variable, d.data(), n), h_, "Print"); }
-        const bool unit_scope = Variable == ActualState || Variable == UnitParameters || Variable == UnitAccessories ||
-                                Variable == IntegerUnitAccessories;
-        const int64_t rows = unit_scope ? (int64_t)NS * UPS : (Variable == GlobalParameters || Variable == IntegerGlobalParameters || Variable == CouplingIndex ? 1 : NS);
-        const int64_t cols = rows > 0 ? n / rows : 0;
-        std::ofstream f(std::string(VariableName(Variable)) + "InSolverObject.txt");
-        f.precision(17);
-        f.flags(std::ios::scientific);
-        for (int64_t r = 0; r < rows; r++) {
-            for (int64_t c = 0; c < cols; c++) {
-                if (is_int) f << iv[c * rows + r]; else f << d[c * rows + r];
-                f << (c + 1 < cols ? "," : "");
-            }
-            f << '\n';
-        }
+    /* Print(ListOfVariables) and Print(ListOfVariables, int), Interface.cuh:1809-1947:
+     * the host mirror to <Variable>InSolverObject.txt (DenseOutput_<n>.txt,
+     * CouplingMatrixInSolverObject_<n>.txt) in the reference's format */
+    void Print(ListOfVariables Variable) { bes_shim::check(bes_print(h_, Variable, 0, nullptr), h_, "Print"); }
+    void Print(ListOfVariables Variable, int SerialNumber) {
+        bes_shim::check(bes_print(h_, Variable, SerialNumber, nullptr), h_, "Print");
     }
 
     void Solve() { bes_shim::check(bes_solve(h_), h_, "Solve"); }

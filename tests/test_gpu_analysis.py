@@ -112,3 +112,49 @@ def test_output_files_have_the_reference_layout(gpu, tmp_path):
     assert lines[s] == f"{s:>4}," + _fmt(up[15, s * n], 18, 10) + "," + "".join(f"{per[s * n + u]:>4}," for u in range(n))
     lines = (tmp_path / "Expansion.csv").read_text().splitlines()
     assert lines[s] == f"{s:>4}," + _fmt(up[16, s * n], 18, 10) + "," + "".join(f"{int(mx[s * n + u]):>4}," for u in range(n))
+
+
+def test_print_files_have_the_reference_layout(gpu, tmp_path):
+    """Print(var) / Print(var, n) (Interface.cuh:1809-1947): width 18, 10 digits,
+    a comma after every value; dense output with its header blocks."""
+    ens = W.c1_ensemble().subset([3, 40])
+    ens.max_steps_per_period = 50_000
+    ps = ens.make_solver(n_dense_output=4)
+    try:
+        ps.SolverOption(S.ListOfSolverOptions.DenseOutputMinimumTimeStep, 0.2)
+        ps.SynchroniseFromHostToDevice(V.All)
+        ps.solve_periods(1, -1)
+        ps.SynchroniseFromDeviceToHost(V.All)
+        ps.InsertSynchronisationPoint()
+        ps.SynchroniseSolver()
+        for v in (V.ActualState, V.TimeDomain, V.IntegerUnitAccessories):
+            ps.Print(v, directory=tmp_path)
+        ps.Print(V.CouplingMatrix, 0, directory=tmp_path)
+        ps.Print(V.DenseOutput, 1, directory=tmp_path)
+        st = ps.get_array(V.ActualState).reshape(2, -1)
+        td = ps.get_array(V.TimeDomain).reshape(2, -1)
+        iu = ps.get_array(V.IntegerUnitAccessories)
+        C = ps.get_array(V.CouplingMatrix)
+        dt = ps.get_array(V.DenseTime).reshape(4, -1)
+        ds = ps.get_array(V.DenseState).reshape(4, 2, -1)
+        di = ps.get_array(V.DenseIndex)
+        up = ps.get_array(V.UnitParameters).reshape(21, -1)
+    finally:
+        ps.close()
+    f18 = lambda v: f"{v:>18.10e}"
+    lines = (tmp_path / "ActualStateInSolverObject.txt").read_text().splitlines()
+    assert len(lines) == 64 and lines[37] == f18(st[0, 37]) + "," + f18(st[1, 37]) + ","
+    lines = (tmp_path / "TimeDomainInSolverObject.txt").read_text().splitlines()
+    assert lines[1] == f18(td[0, 1]) + "," + f18(td[1, 1]) + ","
+    lines = (tmp_path / "IntegerUnitAccessoriesInSolverObject.txt").read_text().splitlines()
+    assert lines[5] == f"{iu[5]:>18}" + ","
+    lines = (tmp_path / "CouplingMatrixInSolverObject_0.txt").read_text().splitlines()
+    assert lines[2] == "".join(f18(C[2 + 32 * j]) + "," for j in range(32))
+    text = (tmp_path / "DenseOutput_1.txt").read_text().split("\n")
+    assert text[0] == "UnitParameters:"
+    assert text[1] == f"{'Serial No.':>18}," + ",".join(f"{'U' + str(u):>18}" for u in range(32))
+    assert text[2] == f"{0:>18}," + ",".join(f18(up[0, 32 + u]) for u in range(32))
+    k = text.index("Time series:")
+    rows = text[k + 2:k + 2 + int(di[1])]
+    assert len(rows) == int(di[1]) >= 1
+    assert rows[0] == f18(dt[0, 1]) + "," + ",".join(f18(ds[0, c, 32 + u]) for u in range(32) for c in range(2))
