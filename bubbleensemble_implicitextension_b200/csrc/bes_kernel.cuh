@@ -24,9 +24,13 @@
  * reductions per BiCG iteration, becomes one column tree per lane over the
  * operator W_ij = (rD_i C_ij) X0_j^2 that is formed once per right-hand side
  * in shared memory (leading dimension 32UG+1: conflict-free row and column
- * reads).  Every scalar of the step control is uniform over the group and
- * held in registers; a single-warp system needs no block barrier at all, a
- * multi-warp system one named barrier per reduction.
+ * reads).  When the launch shares one matrix, it is staged once per CTA
+ * instead; when that matrix is symmetric (a geometry 1/d with the radii as
+ * unit factors), both products become row sums of the same entries -- read
+ * once from shared memory, or for N <= 32 held as a register row for the
+ * whole system.  Every scalar of the step control is uniform over the group
+ * and held in registers; a single-warp system needs no block barrier at all,
+ * a multi-warp system one named barrier per reduction.
  *
  * Arithmetic order (identical in the CPU oracle): sums over units are the
  * halving tree over units padded with zeros to 32UG; the row products use
