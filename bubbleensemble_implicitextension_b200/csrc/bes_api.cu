@@ -67,6 +67,7 @@ struct bes_solver {
     cudaEvent_t sync_event = nullptr, t0 = nullptr, t1 = nullptr;
     int n_systems = 0, ud = 0, nup = 0, nsp = 0, ngp = 0, nigp = 0, nua = 0, niua = 0, nsa = 0, nisa = 0, ne = 0,
         ndo = 0, nc = 1, algorithm = 1;
+    int cbw = 0, cci = 0;   /* coupling storage of the reference: bandwidth, circular indicator */
     std::vector<int32_t> units;
     std::vector<int64_t> unit_offset;
     int64_t total_units = 0;
@@ -514,11 +515,8 @@ bes_status bes_create(const bes_config* c, bes_solver** out) {
                     c->n_system_accessories, c->n_int_system_accessories, c->n_events, BES_MODEL_NAME, BES_MODEL_UD,
                     BES_MODEL_NUP, BES_MODEL_NSP, BES_MODEL_NGP, BES_MODEL_NIGP, BES_MODEL_NUA, BES_MODEL_NIUA,
                     BES_MODEL_NSA, BES_MODEL_NISA, BES_MODEL_NE);
-    if (c->coupling_bandwidth != 0 || c->coupling_circular != 0)
-        return fail(nullptr, BES_ERR_UNSUPPORTED,
-                    "bes_create: banded/circular coupling storage (CBW=%d, CCI=%d) is not supported by the implicit "
-                    "coupling solve (the reference's implicit products assume full storage, "
-                    "ExplicitRungeKutta_Steppers.cuh:660,692)",
+    if (c->coupling_bandwidth < 0 || (c->coupling_circular != 0 && c->coupling_circular != 1))
+        return fail(nullptr, BES_ERR_ARGUMENT, "bes_create: coupling bandwidth %d / circular indicator %d invalid",
                     c->coupling_bandwidth, c->coupling_circular);
     if (c->algorithm != BES_RK4 && c->algorithm != BES_RKCK45)
         return fail(nullptr, BES_ERR_ARGUMENT, "bes_create: unknown algorithm %d", c->algorithm);
@@ -532,6 +530,8 @@ bes_status bes_create(const bes_config* c, bes_solver** out) {
     h->ngp = c->n_global_parameters; h->nigp = c->n_int_global_parameters; h->nua = c->n_unit_accessories;
     h->niua = c->n_int_unit_accessories; h->nsa = c->n_system_accessories; h->nisa = c->n_int_system_accessories;
     h->ne = c->n_events; h->ndo = c->n_dense_output; h->nc = c->n_couplings; h->algorithm = c->algorithm;
+    h->cbw = c->coupling_bandwidth;
+    h->cci = c->coupling_circular;
     h->active = c->n_systems;
     h->units.resize(h->n_systems);
     h->unit_offset.resize(h->n_systems);
@@ -912,12 +912,38 @@ bes_status bes_get_host_global(bes_solver* h, int32_t var, int32_t k, double* v)
     if (!st) *v = get(p, ii);
     return st;
 }
+/* Banded and circular storage (CBW > 0 and/or CCI = 1, Interface.cuh:1010-1070
+ * and ExplicitRungeKutta_Steppers.cuh:586-641): element (row, col) lies on
+ * shifted diagonal (col - row + CBW) mod N, which must be below 2 CBW + 1 when
+ * CBW > 0; with CCI = 1 one value per diagonal serves every row.  The library
+ * keeps the full matrix these formats describe (zero off the band, the
+ * circulant copies filled in), so the implicit products -- which in the
+ * reference index full storage in every mode, Steppers.cuh:660,692 -- see
+ * the coupling the format means. */
 bes_status bes_set_host_coupling(bes_solver* h, int32_t n, int32_t var, int32_t row, int32_t col, double v) {
     if (!h) return BES_ERR_ARGUMENT;
     double* p;
     bes_status st = coupling_slot(h, "SetHost", n, var, row, col, &p);
-    if (!st) *p = v;
-    return st;
+    if (st) return st;
+    if (h->cbw == 0 && h->cci == 0) {
+        *p = v;
+        return BES_OK;
+    }
+    const int m = n / h->nc, dim = h->matrix_dim[m];
+    const int d = ((col - row + h->cbw) % dim + dim) % dim;
+    if (h->cbw > 0 && d > 2 * h->cbw)
+        return fail(h, BES_ERR_INDEX, "SetHost: coupling element (%d, %d) lies outside the band of width %d", row, col,
+                    h->cbw);
+    if (h->cci == 0) {
+        *p = v;
+        return BES_OK;
+    }
+    double* base = p - (row + (int64_t)col * dim);   /* the matrix's (0, 0) */
+    for (int r = 0; r < dim; r++) {
+        const int c = ((r + col - row) % dim + dim) % dim;
+        base[r + (int64_t)c * dim] = v;
+    }
+    return BES_OK;
 }
 bes_status bes_get_host_coupling(bes_solver* h, int32_t n, int32_t var, int32_t row, int32_t col, double* v) {
     if (!h || !v) return BES_ERR_ARGUMENT;

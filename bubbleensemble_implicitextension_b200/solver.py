@@ -325,7 +325,8 @@ class ProblemSolver:
     def __init__(self, n_systems: int, units, *, algorithm: int = Algorithms.RKCK45, n_dense_output: int = 0,
                  n_couplings: int = 1, n_coupling_matrices: int = 1,
                  coupling_matrix_of_system: Optional[Sequence[int]] = None, device: int = 0,
-                 model: Optional[ModelInfo] = None, library: Optional[os.PathLike] = None):
+                 model: Optional[ModelInfo] = None, library: Optional[os.PathLike] = None,
+                 coupling_bandwidth: int = 0, coupling_circular: int = 0):
         self._lib = load_library(library)
         info = ModelInfo()
         _check(self._lib, None, self._lib.bes_model_info_get(ctypes.byref(info)))
@@ -349,6 +350,8 @@ class ProblemSolver:
                   "n_system_accessories", "n_int_system_accessories", "n_events"):
             setattr(cfg, f, getattr(m, f))
         cfg.n_dense_output = n_dense_output
+        cfg.coupling_bandwidth = coupling_bandwidth
+        cfg.coupling_circular = coupling_circular
         cfg.n_couplings = n_couplings
         cfg.algorithm = algorithm
         cfg.n_coupling_matrices = n_coupling_matrices

@@ -135,8 +135,9 @@ typedef struct bes_config {
     int32_t n_events;                  /* NE */
     int32_t n_dense_output;            /* NDO */
     int32_t n_couplings;               /* NC; coupling 0 enters the implicit solve (as in the reference) */
-    int32_t coupling_bandwidth;        /* CBW; must be 0 (full storage) */
-    int32_t coupling_circular;         /* CCI; must be 0 */
+    int32_t coupling_bandwidth;        /* CBW: 0 full storage, > 0 a (wrapping) band of 2 CBW + 1 diagonals */
+    int32_t coupling_circular;         /* CCI: 1 one value per diagonal for every row (circulant); see
+                                          bes_set_host_coupling */
     int32_t algorithm;                 /* BES_RK4 or BES_RKCK45 */
     int32_t n_coupling_matrices;       /* distinct geometries; 1 = one matrix for every system (the reference) */
     const int32_t* coupling_matrix_of_system; /* optional [n_systems]; default s -> 0, or s -> s when
