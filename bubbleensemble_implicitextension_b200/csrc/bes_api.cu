@@ -1351,7 +1351,11 @@ bes_status bes_write_csv(bes_solver* h, int32_t kind, const char* path) {
                     } else if (kind == BES_CSV_PERIOD) {
                         f.width(4); f << ((const int32_t*)h->buf[B_PERIOD].h)[off + u] << ',';
                     } else {
-                        f.width(4); f << (int)((const double*)h->buf[B_MAXACC].h)[off + u] << ',';
+                        /* truncation toward zero as the reference's int array; non-finite or out
+                         * of the int range (undefined for a plain cast) print 0 */
+                        const double a = ((const double*)h->buf[B_MAXACC].h)[off + u];
+                        const int t = (std::isfinite(a) && std::fabs(a) < 2147483647.0) ? (int)a : 0;
+                        f.width(4); f << t << ',';
                     }
                 }
                 f << '\n';
