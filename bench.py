@@ -98,7 +98,7 @@ def parse():
     ap.add_argument("--workload", choices=list(WORKLOADS), default="c1_period1",
                     help="c1_period1 (default, the headline), c2_period1, c3_period1")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample-systems", type=int, default=32)
+    ap.add_argument("--cpu-sample-systems", type=int, default=128)
     ap.add_argument("--systems", type=int, default=0,
                     help="profiling only: integrate an evenly strided subset of S systems (0: all)")
     ap.add_argument("--sweep-window", type=int, default=128, help="c5_sweep: window side within the 1024 grid")
