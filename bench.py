@@ -35,6 +35,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -156,7 +157,7 @@ class Clocks:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+        self.path = Path(tempfile.gettempdir()) / f"bes_clocks_{os.getpid()}.csv"
 
     def start(self):
         try:
@@ -393,7 +394,7 @@ def run_reference(args, rank, world):
     n = args.warmup + args.steps
     clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
     clocks.start()
-    out = ref_io.run(exe, ens, n, -1, ROOT / "gpurun_out" / "ref_bench", tag="bench", timeout=3600,
+    out = ref_io.run(exe, ens, n, -1, Path(tempfile.gettempdir()) / "bes_ref_bench", tag="bench", timeout=3600,
                      restart_each_period=True)
     clk = clocks.stop()
     per = out["period_s"][args.warmup:]

@@ -16,7 +16,7 @@ SourceCodes/CoupledSystems_PerBlock_ExplicitRungeKutta_Steppers.cuh:709-805):
               initial radii, one period;
   cloud_n128  4 systems sharing one random 3-D cloud of 128 bubbles, one period.
 
-Usage (on the GPU machine):  python tests/golden/make_golden.py [outdir]
+Usage (on the GPU machine):  python tests/golden/make_golden.py [outdir] [workdir]
 """
 from __future__ import annotations
 
@@ -33,9 +33,8 @@ from oracle import build_ref, ref_io  # noqa: E402
 from tests.golden import cases  # noqa: E402
 
 
-def main(outdir: Path) -> None:
+def main(outdir: Path, work: Path) -> None:
     outdir.mkdir(parents=True, exist_ok=True)
-    work = ROOT / "gpurun_out" / "golden_work"
     for name, spec in cases.CASES.items():
         ens, run = cases.build(name)
         exe = build_ref.path(spec["units"], spec["harness_ns"], run.get("ndo", 0), True)
@@ -48,4 +47,7 @@ def main(outdir: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path(__file__).resolve().parent)
+    # argv: [output directory for the .npz fixtures] [work directory for the harness's binary files]
+    import tempfile
+    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path(__file__).resolve().parent,
+         Path(sys.argv[2]) if len(sys.argv) > 2 else Path(tempfile.gettempdir()) / "bes_golden_work")

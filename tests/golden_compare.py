@@ -1,6 +1,6 @@
 """Comparison of a run with a golden fixture from the reference's own solver.
 
-Tolerances (north_star): radii within 1e-8 relative at the end of the run
+Tolerances (the parity bar): radii within 1e-8 relative at the end of the run
 and at the saved dense-output times, collapse strength Rmax/Rmin within
 1e-6 relative, identical event counts.  Dense output stores accepted step
 ends, whose times move with the step-size controller (its error estimate

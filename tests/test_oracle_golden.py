@@ -3,7 +3,7 @@
 tests/golden/*.npz were written by tests/golden/make_golden.py, which ran
 the reference's unmodified ProblemSolver (built for sm_100a from its own
 headers by oracle/build_ref.py) on a B200.  This pins the oracle: the
-oracle must reproduce the reference within the north_star tolerances."""
+oracle must reproduce the reference within the parity tolerances."""
 import pytest
 
 from tests import golden_compare
