@@ -230,7 +230,7 @@ def cpu_baseline(ens, n_sample):
     dt = time.perf_counter() - t0
     return {"value": len(systems) / dt, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"CPU oracle (C++ FP64, OpenMP {threads} threads): period 1 of {len(systems)} of the "
-                      f"{ens.n_systems} systems (every {ens.n_systems // len(systems)}th), {dt:.1f} s"}
+                      f"{ens.n_systems} systems (stride {ens.n_systems // len(systems)}), {dt:.1f} s"}
 
 
 def run_b200(args, rank, world, local):
