@@ -23,9 +23,13 @@ Arms:
       (ProblemSolver, built unmodified for sm_100a by oracle/build_ref.py)
       driven through its own API, same workload and metric.
 
-Multi-GPU (torchrun): every rank integrates its own full copy of the
-ensemble (weak scaling, no collective in the data path); the max over ranks
-of the timed region sets the time.
+Multi-GPU (torchrun, one process per GPU): the workload grows with the
+number of GPUs (weak scaling: configuration 1 becomes a 16 x 16N grid, the
+others N times as many systems), a pilot period on an even split measures
+every system's cost, the ensemble is cut into contiguous cost-balanced shards
+(one per rank), and after the solve the result records are gathered on rank 0.
+Systems are independent, so the data path has no collective; the max over
+ranks of the timed region sets the time.
 """
 from __future__ import annotations
 
@@ -79,15 +83,16 @@ WORKLOADS = {
 args_c1_factored = True
 
 
-def make_ensemble(name):
+def make_ensemble(name, world=1):
+    """The workload's ensemble for `world` GPUs (world times the single-GPU size)."""
     from bubbleensemble_implicitextension_b200 import workloads as W
     if name == "c1_period1":
-        return W.c1_ensemble(n_periods=1, reset_at=-1, factored=args_c1_factored)
+        return W.c1_ensemble(n_f=16 * world, n_periods=1, reset_at=-1, factored=args_c1_factored)
     if name == "c2_period1":
-        return W.c2_ensemble(n_periods=1, reset_at=-1)
+        return W.c2_ensemble(n_systems=16384 * world, n_periods=1, reset_at=-1)
     if name == "c3r_period1":
-        return W.c3_radii_ensemble(n_periods=1, reset_at=-1)
-    return W.c3_ensemble(n_periods=1, reset_at=-1)
+        return W.c3_radii_ensemble(n_systems=4096 * world, n_periods=1, reset_at=-1)
+    return W.c3_ensemble(n_systems=4096 * world, n_periods=1, reset_at=-1)
 
 
 def parse():
@@ -119,17 +124,27 @@ def parse():
                     help="1: pick launch shapes with bes_autotune before the warm-up (untimed)")
     ap.add_argument("--warps-per-system", type=int, default=0, choices=[0, 1],
                     help="0: systems above 32 units on 2 or 4 warps (default); 1: one warp per system")
+    ap.add_argument("--bicg-recurrence", type=int, default=1, choices=[0, 1],
+                    help="BiCG recurrence: 1 the single-reduction form (default; within the parity tolerances "
+                         "of the reference's goldens), 0 the reference's own (bit-identical to the oracle's "
+                         "restatement of the reference)")
     return ap.parse_args()
 
 
 def dist_init(n):
     rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         import datetime
 
+        import torch
         import torch.distributed as dist
-        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
-    return rank, world, int(os.environ.get("LOCAL_RANK", "0"))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return rank, world, local
 
 
 def allreduce_max(x, world):
@@ -137,8 +152,20 @@ def allreduce_max(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64)
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend() == "nccl" else torch.device("cpu")
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend() == "nccl" else torch.device("cpu")
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
 
@@ -239,20 +266,32 @@ def run_b200(args, rank, world, local):
     from bubbleensemble_implicitextension_b200 import solver as S
     from bubbleensemble_implicitextension_b200 import workloads as W
 
+    from bubbleensemble_implicitextension_b200 import sharding as SH
+
     V = S.ListOfVariables
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     global args_c1_factored
     args_c1_factored = args.c1_format == "geometry"
-    ens = make_ensemble(args.workload)
-    if 0 < args.systems < ens.n_systems:
-        ens = ens.subset(list(range(0, ens.n_systems, ens.n_systems // args.systems))[:args.systems])
-    # step budget per period: 4.4x the slowest system of c1_period1 and ~4x the 99th percentile of
-    # c2_period1; a system that needs more (the minimum-step cases) is cut short and counted
-    ens.max_steps_per_period = 50_000
+    ens_all = make_ensemble(args.workload, world)
+    if 0 < args.systems < ens_all.n_systems:
+        ens_all = ens_all.subset(list(range(0, ens_all.n_systems, ens_all.n_systems // args.systems))[:args.systems])
+    ens_all.max_steps_per_period = 50_000
+    shard_info = None
+    if world > 1:
+        # pilot (untimed): one period of an even split per rank gives every system's measured cost
+        cost = SH.pilot_costs(ens_all, rank, world, lambda e: solve_counters(e, local, args.bicg_recurrence))
+        bounds = SH.cost_bounds(cost, world)
+        ens = SH.shard(ens_all, bounds, rank)
+        shard_info = {"bounds": bounds.tolist(), "pilot": "one period of an even split per rank (untimed)"}
+    else:
+        ens = ens_all
+    # step budget per period (set on ens_all above): 4.4x the slowest system of c1_period1 and ~4x the
+    # 99th percentile of c2_period1; a system that needs more (the minimum-step cases) is cut short and counted
     ps = ens.make_solver(device=local)
     if args.warps_per_system:
         ps.SolverOption(S.ListOfSolverOptions.WarpsPerSystem, args.warps_per_system)
+    ps.SolverOption(S.ListOfSolverOptions.BiCGRecurrence, args.bicg_recurrence)
     stream = torch.cuda.current_stream(dev)
     ps.set_stream(stream.cuda_stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
@@ -307,11 +346,14 @@ def run_b200(args, rank, world, local):
     total_ms = sum(times)
     max_ms = allreduce_max(total_ms, world)
     ms_per_step = max_ms / args.steps
-    value = world * ens.n_systems * args.steps / (max_ms * 1e-3)
+    value = ens_all.n_systems * args.steps / (max_ms * 1e-3)
 
     # end to end through the public API: host inputs -> H2D -> solve -> D2H of the results
     in_bytes = ens.state.nbytes + init_uacc.nbytes + init_iuacc.nbytes
     out_bytes = in_bytes + 4 * 8 * ens.n_systems + 4 * ens.n_systems
+    # the whole job's copies (every rank copies its shard's share)
+    job_in = int(allreduce_sum(in_bytes, world))
+    job_out = int(allreduce_sum(out_bytes, world))
     e2e_times = []
     for it in range(args.warmup + args.steps):
         flush.zero_()
@@ -332,7 +374,14 @@ def run_b200(args, rank, world, local):
         if it >= args.warmup:
             e2e_times.append(time.perf_counter() - t0)
     e2e_max = allreduce_max(sum(e2e_times), world)
-    e2e_value = world * ens.n_systems * args.steps / e2e_max
+    e2e_value = ens_all.n_systems * args.steps / e2e_max
+    # the shards' result records on rank 0 (after the timed regions)
+    c_last = ps.counters()
+    local_rec = {"state": ps.get_array(V.ActualState).reshape(2, -1), "uacc": ps.get_array(V.UnitAccessories).reshape(64, -1),
+                 "iuacc": ps.get_array(V.IntegerUnitAccessories).reshape(1, -1),
+                 "n_accepted": c_last["accepted"], "n_rejected": c_last["rejected"], "n_bicg_iter": c_last["bicg"],
+                 "n_rhs": c_last["rhs"], "status": c_last["status"]}
+    gathered = SH.gather_results(local_rec, rank, world)
     peak = S.measure_fp64_peak(local)
     ps.close()
     if rank != 0:
@@ -343,24 +392,28 @@ def run_b200(args, rank, world, local):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": DATA,
-        "config": {"workload": WORKLOADS[args.workload], "systems": ens.n_systems,
+        "config": {"workload": WORKLOADS[args.workload], "systems": ens_all.n_systems,
                    "units_per_system": int(ens.units[0]) if len(set(ens.units.tolist())) == 1 else "mixed",
                    "total_units": ens.total_units,
                    "periods_per_step": 1,
                    "coupling_input": ("shared symmetric geometry G = 1/d with unit factors R^-2, R^3"
                                       if ens.coupling_row_scale is not None else "per-ensemble matrix as given"),
                    "warps_per_system": "one" if args.warps_per_system else "2 or 4 above 32 units",
+                   "bicg_recurrence": ("single reduction per iteration (BiCGRecurrence 1)" if args.bicg_recurrence
+                                       else "the reference's (BiCGRecurrence 0)"),
                    "launch_shapes": tuned if tuned else "heuristic",
                    "l2": "flushed between timed steps (256 MiB write, untimed)",
-                   "parallelism": f"{world} independent ensemble replica(s), one per GPU"},
+                   "parallelism": (f"{world} contiguous cost-balanced shards of one {ens_all.n_systems}-system ensemble, "
+                                   "one per GPU, results gathered on rank 0" if world > 1 else "one GPU"),
+                   "shards": shard_info,
+                   "gathered_systems": int(len(gathered["status"]))},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None,
                      "traffic": read_traffic() if args.workload == "c1_period1" else None,
                      "peak_source": "measured live: bes_measure_fp64_peak FMA-throughput loop (no FP64 figure in "
                                     "MEASURED_PEAKS.json)",
                      "flops_per_launch": flops, "kernel": "bes::bes_ensemble_kernel (all classes of the launch plan)"},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(in_bytes),
-                "d2h_bytes_per_step": int(out_bytes)},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": job_in, "d2h_bytes_per_step": job_out},
         "gpu_launches": launches,
         "clocks": clk,
         "counters": {"attempted_steps": int(attempted.sum()), "max_attempted_steps": int(attempted.max()),
@@ -371,6 +424,24 @@ def run_b200(args, rank, world, local):
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(ens, args.cpu_sample_systems)
     return line
+
+
+def solve_counters(ens, device, bicg_recurrence):
+    """One period of `ens` through the library; per-system counters (the sharding pilot)."""
+    from bubbleensemble_implicitextension_b200 import solver as S
+    V = S.ListOfVariables
+    ps = ens.make_solver(device=device)
+    try:
+        ps.SolverOption(S.ListOfSolverOptions.BiCGRecurrence, bicg_recurrence)
+        ps.SynchroniseFromHostToDevice(V.All)
+        ps.solve_periods(1, -1)
+        ps.SynchroniseFromDeviceToHost(V.Counters)
+        ps.InsertSynchronisationPoint()
+        ps.SynchroniseSolver()
+        c = ps.counters()
+        return {"n_accepted": c["accepted"], "n_rejected": c["rejected"]}
+    finally:
+        ps.close()
 
 
 def run_reference(args, rank, world):

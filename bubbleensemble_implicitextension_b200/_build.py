@@ -1,8 +1,8 @@
 """In-tree build of the CUDA library ``libbes.so`` for sm_100a.
 
 Each kernel layout class (1, 2 or 4 units per lane on one warp; one unit
-per lane on 2 or 4 warps) is its own translation unit, so the objects
-compile in parallel; the shared library lands next to this
+per lane on 2 or 4 warps) with each BiCG recurrence is its own translation
+unit, so the objects compile in parallel; the shared library lands next to this
 file so it travels with the source tree.
 """
 from __future__ import annotations
@@ -19,8 +19,8 @@ INCLUDE = PKG.parent / "include"
 BUILD = PKG / "_build"
 LIB = PKG / "libbes.so"
 
-SOURCES = ["bes_api.cu", "bes_launch.cu", "bes_peak.cu", "bes_noalloc.cu", "bes_mlp.cu",
-           "bes_kernel_u1.cu", "bes_kernel_u2.cu", "bes_kernel_u4.cu", "bes_kernel_g2.cu", "bes_kernel_g4.cu"]
+KERNEL_UNITS = [f"bes_kernel_{c}{r}.cu" for c in ("u1", "u2", "u4", "g2", "g4") for r in ("", "_r1")]
+SOURCES = ["bes_api.cu", "bes_launch.cu", "bes_peak.cu", "bes_noalloc.cu", "bes_mlp.cu", *KERNEL_UNITS]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",

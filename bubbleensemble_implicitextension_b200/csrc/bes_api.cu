@@ -114,6 +114,7 @@ struct bes_solver {
     bool graph_dirty = true;
     int use_graph = 1;
     int warps_per_system = 0;   /* 0: multi-warp systems above 32 units; 1: one warp per system */
+    int bicg_recurrence = 0;    /* 0: the reference's BiCG recurrence; 1: the single-reduction form */
     int tuned_wpb[3] = {0, 0, 0};      /* per size class, set by bes_autotune (0: not tuned) */
     int tuned_wps[3] = {-1, -1, -1};   /* per size class, set by bes_autotune (-1: not tuned) */
     float last_ms = 0.f;
@@ -382,7 +383,7 @@ struct ClassLaunch {
 /* launch shape of one class (no stream work: safe before a capture) */
 bes_status plan_shape(bes_solver* h, int cls, int warps_per_system, int requested_wpb, ClassLaunch* L) {
     const bes::Variant v = bes::class_variant(cls, h->class0_all32, h->shared_coupling && h->class_shared[cls],
-                                         warps_per_system, h->class_symmetric[cls]);
+                                         warps_per_system, h->class_symmetric[cls], h->bicg_recurrence);
     const int count = h->class_count[cls];
     if (bes::max_warps_per_block(v) < v.G)
         return fail(h, BES_ERR_CUDA, "solver kernel variant (U=%d, G=%d) does not fit in shared memory", v.U, v.G);
@@ -727,6 +728,11 @@ bes_status bes_solver_option(bes_solver* h, int32_t option, double value) {
                 return fail(h, BES_ERR_ARGUMENT, "SolverOption: WarpsPerSystem must be 0 (automatic) or 1");
             h->warps_per_system = (int)value;
             for (int c = 0; c < 3; c++) h->tuned_wps[c] = -1;
+            break;
+        case BES_OPT_BICG_RECURRENCE:
+            if (!(value == 0.0 || value == 1.0))
+                return fail(h, BES_ERR_ARGUMENT, "SolverOption: BiCGRecurrence must be 0 (reference) or 1 (single reduction)");
+            h->bicg_recurrence = (int)value;
             break;
         default:
             return fail(h, BES_ERR_OPTION, "SolverOption: option %d needs an index argument or is not applicable", option);
@@ -1418,7 +1424,7 @@ bes_status bes_autotune(bes_solver* h, int32_t n_periods, int64_t step_cap, bes_
         for (int wps = 0; wps <= (cls == 0 ? 0 : 1) && !st; wps++) {
             const bes::Variant v = bes::class_variant(cls, h->class0_all32,
                                                       h->shared_coupling && h->class_shared[cls], wps,
-                                                      h->class_symmetric[cls]);
+                                                      h->class_symmetric[cls], h->bicg_recurrence);
             const int cap = bes::max_warps_per_block(v);
             for (int wpb = v.G; wpb <= cap && !st; wpb *= 2) {
                 ClassLaunch L;

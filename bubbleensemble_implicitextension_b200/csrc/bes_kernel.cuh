@@ -70,6 +70,9 @@ constexpr int NSPa = NSP > 0 ? NSP : 1;
 constexpr int NSAa = NSA > 0 ? NSA : 1;
 constexpr int NISAa = NISA > 0 ? NISA : 1;
 constexpr unsigned FULL = 0xffffffffu;
+/* one group-exchange buffer: two values per unit of the largest group
+ * (128 units) and one flag word per warp, padded to 16-byte multiples */
+constexpr int XCH_BUF = 2 * 128 + 8;
 
 /* Shared-memory doubles per system (G warps, U units per lane, NMAX = 32 U G
  * units): one NMAX x (NMAX+1) matrix region (the operator W with the
@@ -85,7 +88,7 @@ struct WarpSmem {
     static constexpr int LDW = NMAX + 1;
     static constexpr int W_DOUBLES = NMAX * LDW;
     static constexpr int VEC_DOUBLES = 6 * NMAX;
-    static constexpr int XCH_DOUBLES = G > 1 ? 4 * NMAX : 0; /* two buffers of two values per unit */
+    static constexpr int XCH_DOUBLES = G > 1 ? 2 * XCH_BUF : 0; /* two buffers of two values per unit + flags */
     static constexpr int SYS_DOUBLES = NSPa + NSAa + NISAa;  /* ints stored in double slots */
     static constexpr int UP_DOUBLES = U == 1 ? NMAX * NUPa : 0; /* unit parameters (one unit per lane) */
     static constexpr int WT_DOUBLES = U == 1 && G == 1 ? NMAX * LDW : 0;  /* operator W of the register variants */
@@ -108,7 +111,7 @@ struct SharedCSmem {
     static constexpr int NMAX = 32 * U * G;
     static constexpr int LDC = NMAX + 2;
     static constexpr int C_DOUBLES = NMAX * LDC;
-    static constexpr int XCH_DOUBLES = G > 1 ? 4 * NMAX : 0;
+    static constexpr int XCH_DOUBLES = G > 1 ? 2 * XCH_BUF : 0;
     static constexpr int UP_DOUBLES = U == 1 ? NMAX * NUPa : 0; /* unit parameters (one unit per lane) */
     static constexpr int WARP_DOUBLES = (5 * NMAX + XCH_DOUBLES + NSPa + NSAa + NISAa + UP_DOUBLES + 31) / 32 * 32;
     static constexpr int C_BYTES = C_DOUBLES * 8;
@@ -189,7 +192,8 @@ __device__ __forceinline__ void grp_sync(const Sys<U, G>& S) {
 
 template <int U, int G>
 __device__ __forceinline__ double* grp_buffer(const Sys<U, G>& S) {
-    double* b = S.xch + (S.xsel & 1) * (2 * 32 * U * G);
+    static_assert(2 * 32 * U * G + G <= XCH_BUF, "exchange buffer too small");
+    double* b = S.xch + (S.xsel & 1) * XCH_BUF;
     S.xsel++;
     return b;
 }
@@ -335,9 +339,226 @@ __device__ __forceinline__ int grp_resolve_int(const Sys<U, G>& S, int before, i
     return (int)grp_resolve<U, G>(S, (double)before, (double)after_lane, first_unit);
 }
 
+/* Two sums over all 32U units of the warp, each in halving-tree order (the
+ * shuffles of the two butterflies interleave); every lane gets both. */
+template <int U>
+__device__ __forceinline__ void warp_tree_sum2(const double (&v)[U], const double (&w)[U], double& sv, double& sw) {
+    double a[U], b[U];
+#pragma unroll
+    for (int m = 0; m < U; m++) { a[m] = v[m]; b[m] = w[m]; }
+#pragma unroll
+    for (int h = U / 2; h >= 1; h /= 2)
+#pragma unroll
+        for (int m = 0; m < h; m++) { a[m] = a[m] + a[m + h]; b[m] = b[m] + b[m + h]; }
+    double s = a[0], t = b[0];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        const double so = __shfl_xor_sync(FULL, s, o), to = __shfl_xor_sync(FULL, t, o);
+        s = s + so;
+        t = t + to;
+    }
+    sv = s;
+    sw = t;
+}
+
+/* two sums over the system's units in one group exchange (each bit-identical to grp_tree_sum) */
+template <int U, int G>
+__device__ __forceinline__ void grp_tree_sum2(const Sys<U, G>& S, const double (&v)[U], const double (&w)[U],
+                                              double& sv, double& sw) {
+    if constexpr (G == 1) {
+        warp_tree_sum2<U>(v, w, sv, sw);
+    } else {
+        double in[2][U], a[2][U * G];
+#pragma unroll
+        for (int m = 0; m < U; m++) { in[0][m] = v[m]; in[1][m] = w[m]; }
+        grp_gather<U, G, 2>(S, in, a);
+        warp_tree_sum2<U * G>(a[0], a[1], sv, sw);
+    }
+}
+
+/* the BiCG exit test alone: fmax-tree maximum of x over the system below lim
+ * (same decision and NaN rule as grp_sum_max_below) */
+template <int U, int G>
+__device__ __forceinline__ bool grp_max_below(const Sys<U, G>& S, const double (&x)[U], double lim) {
+    bool ok = true, seen = false;
+#pragma unroll
+    for (int m = 0; m < U; m++) {
+        ok = ok && (isnan(x[m]) || x[m] < lim);
+        seen = seen || !isnan(x[m]);
+    }
+    const bool wok = __all_sync(FULL, ok), wseen = __any_sync(FULL, seen);
+    if constexpr (G == 1) {
+        return wok && wseen;
+    } else {
+        double f[G];
+        grp_share(S, (wok ? 1.0 : 0.0) + (wseen ? 2.0 : 0.0), f);
+        bool all_ok = true, any_seen = false;
+#pragma unroll
+        for (int w = 0; w < G; w++) {
+            all_ok = all_ok && (f[w] == 1.0 || f[w] == 3.0);
+            any_seen = any_seen || f[w] >= 2.0;
+        }
+        return all_ok && any_seen;
+    }
+}
+
+/* exit test and two sums in one exchange (multi-warp groups) */
+template <int U, int G>
+__device__ __forceinline__ bool grp_sum2_max_below(const Sys<U, G>& S, const double (&x)[U], const double (&y)[U],
+                                                   const double (&z)[U], double lim, double& ysum, double& zsum) {
+    static_assert(G > 1, "single warps test by votes");
+    bool ok = true, seen = false;
+#pragma unroll
+    for (int m = 0; m < U; m++) {
+        ok = ok && (isnan(x[m]) || x[m] < lim);
+        seen = seen || !isnan(x[m]);
+    }
+    const bool wok = __all_sync(FULL, ok), wseen = __any_sync(FULL, seen);
+    double* buf = grp_buffer(S);
+    constexpr int NB = U * G;
+#pragma unroll
+    for (int m = 0; m < U; m++) {
+        buf[(G * m + S.wis) * 32 + S.lane] = y[m];
+        buf[32 * NB + (G * m + S.wis) * 32 + S.lane] = z[m];
+    }
+    if (S.lane == 0) buf[64 * NB + S.wis] = (wok ? 1.0 : 0.0) + (wseen ? 2.0 : 0.0);
+    grp_sync(S);
+    double a[NB], b[NB];
+#pragma unroll
+    for (int k = 0; k < NB; k++) { a[k] = buf[k * 32 + S.lane]; b[k] = buf[32 * NB + k * 32 + S.lane]; }
+    warp_tree_sum2<NB>(a, b, ysum, zsum);
+    bool all_ok = true, any_seen = false;
+#pragma unroll
+    for (int w = 0; w < G; w++) {
+        const double f = buf[64 * NB + w];
+        all_ok = all_ok && (f == 1.0 || f == 3.0);
+        any_seen = any_seen || f >= 2.0;
+    }
+    return all_ok && any_seen;
+}
+
+/* ---------------------------------------------------------------------------
+ * BiCG iterations (Steppers.cuh:508-561) on a system whose residual r
+ * (r~ = r) and start x are set.  apply(v, vt, q, qt) forms q = A v and
+ * q~ = A^T vt, zero for slots beyond the system's units.
+ *
+ * REC = 0: the reference's recurrence -- per iteration the products of the
+ * search directions, then alpha from one reduction and the exit test with the
+ * next rho from a second.
+ * REC = 1: the single-reduction form of the same iterates.  The products of
+ * the residuals w = A r, w~ = A^T r~ come first; one reduction gives
+ * rho = r.r~ and mu = r~.w together; then
+ *   beta = rho / rho_prev, sigma = mu - beta^2 sigma_prev,
+ *   p = r + beta p, p~ = r~ + beta p~, q = w + beta q, q~ = w~ + beta q~,
+ *   alpha = rho / sigma,
+ * so q = A p, q~ = A^T p~ and sigma = p~.A p (its cross terms equal
+ * -rho/alpha_prev = -beta sigma_prev each, by the biorthogonality of the
+ * residuals).  Same exits as the reference (|rho| < 1e-6 before the first
+ * update, max |r| < 1e-6 after each, at most bicg_max_iter updates); a
+ * single warp tests by votes right after the update, a group folds the test
+ * into the next reduction's exchange (the test sees the same r).  Returns the
+ * completed iterations; sets capped when the cap ended the loop. */
+template <int U, int G, int REC, class Apply>
+__device__ __forceinline__ int bicg_iterate(const Sys<U, G>& S, const DeviceProblem& P, double (&r)[U],
+                                            double (&x)[U], Apply&& apply, bool& capped) {
+    double rt[U], p[U], pt[U], q[U], qt[U], prod[U], ar[U];
+#pragma unroll
+    for (int m = 0; m < U; m++) { rt[m] = r[m]; p[m] = 0.0; pt[m] = 0.0; ar[m] = 0.0; }
+    int done = 0;
+    bool exited = false;
+    if constexpr (REC == 0) {
+#pragma unroll
+        for (int m = 0; m < U; m++) prod[m] = r[m] * rt[m];
+        double rho1 = grp_tree_sum<U, G>(S, prod);
+        double rho2 = 0.0;
+        for (int iter = 1; iter <= P.bicg_max_iter; iter++) {
+            if (iter == 1) {
+#pragma unroll
+                for (int m = 0; m < U; m++) { p[m] = r[m]; pt[m] = rt[m]; }
+                if (fabs(rho1) < 1e-6) { exited = true; break; }
+            } else {
+                const double beta = rho1 / rho2;
+#pragma unroll
+                for (int m = 0; m < U; m++) {
+                    p[m] = fma(beta, p[m], r[m]);
+                    pt[m] = fma(beta, pt[m], rt[m]);
+                }
+            }
+            apply(p, pt, q, qt);
+#pragma unroll
+            for (int m = 0; m < U; m++) prod[m] = pt[m] * q[m];
+            const double alpha = rho1 / grp_tree_sum<U, G>(S, prod);
+#pragma unroll
+            for (int m = 0; m < U; m++) {
+                x[m] = fma(alpha, p[m], x[m]);
+                r[m] = fma(-alpha, q[m], r[m]);
+                rt[m] = fma(-alpha, qt[m], rt[m]);
+                ar[m] = fabs(r[m]);
+                prod[m] = r[m] * rt[m];
+            }
+            double rho_next;
+            const bool small = grp_sum_max_below<U, G>(S, ar, prod, 1e-6, rho_next);
+            rho2 = rho1;
+            done++;
+            if (small) { exited = true; break; }
+            rho1 = rho_next;
+        }
+    } else {
+        double w[U], wt[U], rw[U];
+        double sigma = 0.0, rho_prev = 0.0;
+        for (int iter = 1; iter <= P.bicg_max_iter; iter++) {
+            apply(r, rt, w, wt);
+#pragma unroll
+            for (int m = 0; m < U; m++) { prod[m] = r[m] * rt[m]; rw[m] = rt[m] * w[m]; }
+            double rho, mu;
+            if constexpr (G == 1) {
+                grp_tree_sum2<U, G>(S, prod, rw, rho, mu);
+            } else {
+                if (iter == 1) grp_tree_sum2<U, G>(S, prod, rw, rho, mu);
+                else if (grp_sum2_max_below<U, G>(S, ar, prod, rw, 1e-6, rho, mu)) { exited = true; break; }
+            }
+            if (iter == 1) {
+                if (fabs(rho) < 1e-6) { exited = true; break; }
+#pragma unroll
+                for (int m = 0; m < U; m++) { p[m] = r[m]; pt[m] = rt[m]; q[m] = w[m]; qt[m] = wt[m]; }
+                sigma = mu;
+            } else {
+                const double beta = rho / rho_prev;
+                sigma = fma(-(beta * beta), sigma, mu);
+#pragma unroll
+                for (int m = 0; m < U; m++) {
+                    p[m] = fma(beta, p[m], r[m]);
+                    pt[m] = fma(beta, pt[m], rt[m]);
+                    q[m] = fma(beta, q[m], w[m]);
+                    qt[m] = fma(beta, qt[m], wt[m]);
+                }
+            }
+            const double alpha = rho / sigma;
+            rho_prev = rho;
+#pragma unroll
+            for (int m = 0; m < U; m++) {
+                x[m] = fma(alpha, p[m], x[m]);
+                r[m] = fma(-alpha, q[m], r[m]);
+                rt[m] = fma(-alpha, qt[m], rt[m]);
+                ar[m] = fabs(r[m]);
+            }
+            done++;
+            if constexpr (G == 1) {
+                if (grp_max_below<U, G>(S, ar, 1e-6)) { exited = true; break; }
+            }
+        }
+        if constexpr (G > 1) {
+            /* the update that used up the cap has not been tested yet */
+            if (!exited && done > 0 && done == P.bicg_max_iter && grp_max_below<U, G>(S, ar, 1e-6)) exited = true;
+        }
+    }
+    if (!exited) capped = true;
+    return done;
+}
+
 /* ---------------------------------------------------------------------------
  * Coupled right-hand side of the whole system (Steppers.cuh:432-562). */
-template <int U, int G>
+template <int U, int G, int REC>
 __device__ __forceinline__ int coupled_rhs(const Sys<U, G>& S, const DeviceProblem& P, double T,
                                            double (&Xs)[U][UD], double (&F)[U][UD],
                                            double (&up)[U][NUPa], double (&ua)[U][NUAa],
@@ -345,7 +566,7 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U, G>& S, const DeviceProbl
     constexpr int NMAX = WarpSmem<U, G>::NMAX;
     constexpr int LDW = WarpSmem<U, G>::LDW;
     const int N = S.N;
-    double xu[U], rd[U], r[U], rt[U], x[U], p[U], pt[U];
+    double xu[U], rd[U], r[U], x[U];
     grp_sync(S);
 #pragma unroll
     for (int m = 0; m < U; m++) {
@@ -403,40 +624,18 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U, G>& S, const DeviceProbl
         } else {
             r[m] = 0.0;
         }
-        rt[m] = r[m];
         x[m] = xu[m];
-        p[m] = 0.0;
-        pt[m] = 0.0;
     }
-    double prod[U];
-#pragma unroll
-    for (int m = 0; m < U; m++) prod[m] = r[m] * rt[m];
-    double rho1 = grp_tree_sum<U, G>(S, prod);
-    double rho2 = 0.0;
-    int done = 0;
-    bool exited = false;
-    for (int iter = 1; iter <= P.bicg_max_iter; iter++) {
-        if (iter == 1) {
-#pragma unroll
-            for (int m = 0; m < U; m++) { p[m] = r[m]; pt[m] = rt[m]; }
-            if (fabs(rho1) < 1e-6) { exited = true; break; }
-        } else {
-            double beta = rho1 / rho2;
-#pragma unroll
-            for (int m = 0; m < U; m++) {
-                p[m] = fma(beta, p[m], r[m]);
-                pt[m] = fma(beta, pt[m], rt[m]);
-            }
-        }
+    /* q = A v (row sums of W), q~ = A^T vt (column tree of W) */
+    auto apply = [&](const double (&v)[U], const double (&vt)[U], double (&q)[U], double (&qt)[U]) {
         grp_sync(S);
 #pragma unroll
         for (int m = 0; m < U; m++) {
             const int i = S.unit(m);
-            S.vp[i] = p[m];
-            S.vpt[i] = pt[m];
+            S.vp[i] = v[m];
+            S.vpt[i] = vt[m];
         }
         grp_sync(S);
-        double q[U], qt[U];
 #pragma unroll
         for (int m = 0; m < U; m++) {
             const int i = S.unit(m);
@@ -453,37 +652,18 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U, G>& S, const DeviceProbl
                 if (j < N) q0 = fma(Wi[j * LDW], S.vp[j], q0);
                 if (j + 1 < N) q1 = fma(Wi[(j + 1) * LDW], S.vp[j + 1], q1);
                 if (j + 2 < N) q2 = fma(Wi[(j + 2) * LDW], S.vp[j + 2], q2);
-                q[m] = p[m] + ((q0 + q1) + (q2 + q3));
+                q[m] = v[m] + ((q0 + q1) + (q2 + q3));
                 const double* Wc = S.W + (int64_t)i * LDW;
                 const double* vpt = S.vpt;
                 auto leaf = [&](int j) -> double { return j < N ? Wc[j] * vpt[j] : 0.0; };
-                qt[m] = pt[m] + TreeSum<1, NMAX>::run(0, leaf);
+                qt[m] = vt[m] + TreeSum<1, NMAX>::run(0, leaf);
             } else {
                 q[m] = 0.0;
                 qt[m] = 0.0;
             }
         }
-#pragma unroll
-        for (int m = 0; m < U; m++) prod[m] = pt[m] * q[m];
-        double alpha = rho1 / grp_tree_sum<U, G>(S, prod);
-        double ar[U];
-#pragma unroll
-        for (int m = 0; m < U; m++) {
-            x[m] = fma(alpha, p[m], x[m]);
-            r[m] = fma(-alpha, q[m], r[m]);
-            rt[m] = fma(-alpha, qt[m], rt[m]);
-            ar[m] = fabs(r[m]);
-        }
-#pragma unroll
-        for (int m = 0; m < U; m++) prod[m] = r[m] * rt[m];
-        double rho_next;
-        const bool small = grp_sum_max_below<U, G>(S, ar, prod, 1e-6, rho_next);
-        rho2 = rho1;
-        done++;
-        if (small) { exited = true; break; }
-        rho1 = rho_next;
-    }
-    if (!exited) capped = true;
+    };
+    const int done = bicg_iterate<U, G, REC>(S, P, r, x, apply, capped);
 #pragma unroll
     for (int m = 0; m < U; m++) F[m][IC] = x[m];
     return done;
@@ -498,7 +678,7 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U, G>& S, const DeviceProbl
  * (padded, leading dimension 33: row and column reads are conflict-free),
  * staged once per system.  NFIX = 32 drops the N guards for full warps.
  * Same arithmetic, in the same order, as the shared-memory variant. */
-template <int NFIX>
+template <int NFIX, int REC>
 __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DeviceProblem& P, double T,
                                                 double (&Xs)[1][UD], double (&F)[1][UD],
                                                 double (&up)[1][NUPa], double (&ua)[1][NUAa],
@@ -561,27 +741,13 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
         const double ax = fma(rd, (as[0] + as[1]) + (as[2] + as[3]), xu);
         r = b - ax;
     }
-    double rt = r, x = xu, p = 0.0, pt = 0.0;
-    double prod[1] = {r * rt};
-    double rho1 = warp_tree_sum<1>(prod);
-    double rho2 = 0.0;
-    int done = 0;
-    bool exited = false;
     const double2* vp2 = reinterpret_cast<const double2*>(S.vp);
     const double2* vpt2 = reinterpret_cast<const double2*>(S.vpt);
-    for (int iter = 1; iter <= P.bicg_max_iter; iter++) {
-        if (iter == 1) {
-            p = r;
-            pt = rt;
-            if (fabs(rho1) < 1e-6) { exited = true; break; }
-        } else {
-            const double beta = rho1 / rho2;
-            p = fma(beta, p, r);
-            pt = fma(beta, pt, rt);
-        }
+    /* q = A v (row of W in registers), q~ = A^T vt (column of W from shared memory) */
+    auto apply = [&](const double (&v)[1], const double (&vt)[1], double (&qo)[1], double (&qto)[1]) {
         __syncwarp();
-        S.vp[i] = p;
-        S.vpt[i] = pt;
+        S.vp[i] = v[0];
+        S.vpt[i] = vt[0];
         __syncwarp();
         double qs[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
@@ -590,7 +756,7 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
             if (NFIX != 0 || j < N) qs[j & 3] = fma(wr[j], a.x, qs[j & 3]);
             if (NFIX != 0 || j + 1 < N) qs[(j + 1) & 3] = fma(wr[j + 1], a.y, qs[(j + 1) & 3]);
         }
-        double q = p + ((qs[0] + qs[1]) + (qs[2] + qs[3]));
+        double q = v[0] + ((qs[0] + qs[1]) + (qs[2] + qs[3]));
         /* column i of W from shared memory (lane-consecutive rows, conflict-free);
          * first tree level t_k + t_{k+16} on the loads, then the halving tree over 16 */
         const double* Wc = Wt + i * LDC;
@@ -602,23 +768,14 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
             u[k + 1] = Wc[k + 1] * lo.y + Wc[k + 17] * hi.y;
         }
         auto leaf = [&](int k) -> double { return u[k]; };
-        double qt = pt + TreeSum<1, 16>::run(0, leaf);
+        double qt = vt[0] + TreeSum<1, 16>::run(0, leaf);
         if (!valid) { q = 0.0; qt = 0.0; }
-        prod[0] = pt * q;
-        const double alpha = rho1 / warp_tree_sum<1>(prod);
-        x = fma(alpha, p, x);
-        r = fma(-alpha, q, r);
-        rt = fma(-alpha, qt, rt);
-        double ar[1] = {fabs(r)};
-        prod[0] = r * rt;
-        double rho_next;
-        const bool small = grp_sum_max_below<1, 1>(S, ar, prod, 1e-6, rho_next);
-        rho2 = rho1;
-        done++;
-        if (small) { exited = true; break; }
-        rho1 = rho_next;
-    }
-    if (!exited) capped = true;
+        qo[0] = q;
+        qto[0] = qt;
+    };
+    double rr[1] = {r}, xx[1] = {xu};
+    const int done = bicg_iterate<1, 1, REC>(S, P, rr, xx, apply, capped);
+    const double x = xx[0];
     F[0][IC] = x;
     return done;
 }
@@ -634,7 +791,7 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
  * with G row sums as four interleaved fma chains and G column sums in the
  * halving-tree order over 32UG; the oracle's shared-matrix association
  * computes the same (a = b = 1 reproduces the unscaled products bit for bit). */
-template <int U, int G, bool SYM>
+template <int U, int G, bool SYM, int REC>
 __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const DeviceProblem& P, double T,
                                                    double (&Xs)[U][UD], double (&F)[U][UD],
                                                    double (&up)[U][NUPa], double (&ua)[U][NUAa],
@@ -645,7 +802,7 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const Dev
     constexpr int H = NMAX / 2;
     const int N = S.N;
     /* with C = diag(a) G diag(b): x1 holds u = b X1sq (applied before G), rd holds v = rD a (after G) */
-    double xu[U], rd[U], x1[U], r[U], rt[U], x[U], p[U], pt[U];
+    double xu[U], rd[U], x1[U], r[U], x[U];
     grp_sync(S);
 #pragma unroll
     for (int m = 0; m < U; m++) {
@@ -748,37 +905,16 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const Dev
         } else {
             r[m] = 0.0;
         }
-        rt[m] = r[m];
         x[m] = xu[m];
-        p[m] = 0.0;
-        pt[m] = 0.0;
     }
-    double prod[U];
-#pragma unroll
-    for (int m = 0; m < U; m++) prod[m] = r[m] * rt[m];
-    double rho1 = grp_tree_sum<U, G>(S, prod);
-    double rho2 = 0.0;
-    int done = 0;
-    bool exited = false;
-    for (int iter = 1; iter <= P.bicg_max_iter; iter++) {
-        if (iter == 1) {
-#pragma unroll
-            for (int m = 0; m < U; m++) { p[m] = r[m]; pt[m] = rt[m]; }
-            if (fabs(rho1) < 1e-6) { exited = true; break; }
-        } else {
-            const double beta = rho1 / rho2;
-#pragma unroll
-            for (int m = 0; m < U; m++) {
-                p[m] = fma(beta, p[m], r[m]);
-                pt[m] = fma(beta, pt[m], rt[m]);
-            }
-        }
+    /* q = A v = v + rD a (G (b X1sq v)), q~ = A^T vt = vt + b X1sq (G^T (rD a vt)) */
+    auto apply = [&](const double (&v)[U], const double (&vt)[U], double (&q)[U], double (&qt)[U]) {
         grp_sync(S);
 #pragma unroll
         for (int m = 0; m < U; m++) {
             const int i = S.unit(m);
-            S.vp[i] = x1[m] * p[m];    /* z  = X1sq p  */
-            S.vpt[i] = rd[m] * pt[m];  /* z~ = rD p~   */
+            S.vp[i] = x1[m] * v[m];    /* z  = X1sq v  */
+            S.vpt[i] = rd[m] * vt[m];  /* z~ = rD vt   */
         }
         grp_sync(S);
         double qs[U], qts[U];
@@ -815,33 +951,14 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const Dev
             qts[m] = TreeSum<1, 32>::run(0, leaf);
         }
         }
-        double q[U], qt[U];
 #pragma unroll
         for (int m = 0; m < U; m++) {
-            const bool v = S.unit(m) < N;
-            q[m] = v ? fma(rd[m], qs[m], p[m]) : 0.0;
-            qt[m] = v ? fma(x1[m], qts[m], pt[m]) : 0.0;
+            const bool vld = S.unit(m) < N;
+            q[m] = vld ? fma(rd[m], qs[m], v[m]) : 0.0;
+            qt[m] = vld ? fma(x1[m], qts[m], vt[m]) : 0.0;
         }
-#pragma unroll
-        for (int m = 0; m < U; m++) prod[m] = pt[m] * q[m];
-        const double alpha = rho1 / grp_tree_sum<U, G>(S, prod);
-        double ar[U];
-#pragma unroll
-        for (int m = 0; m < U; m++) {
-            x[m] = fma(alpha, p[m], x[m]);
-            r[m] = fma(-alpha, q[m], r[m]);
-            rt[m] = fma(-alpha, qt[m], rt[m]);
-            ar[m] = fabs(r[m]);
-            prod[m] = r[m] * rt[m];
-        }
-        double rho_next;
-        const bool small = grp_sum_max_below<U, G>(S, ar, prod, 1e-6, rho_next);
-        rho2 = rho1;
-        done++;
-        if (small) { exited = true; break; }
-        rho1 = rho_next;
-    }
-    if (!exited) capped = true;
+    };
+    const int done = bicg_iterate<U, G, REC>(S, P, r, x, apply, capped);
 #pragma unroll
     for (int m = 0; m < U; m++) F[m][IC] = x[m];
     return done;
@@ -854,7 +971,7 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const Dev
  * formed per right-hand side -- and both BiCG products are row sums of that
  * row against broadcast vectors, with the unit factors a, b as in
  * coupled_rhs_sharedc<.., SYM = true> and the same arithmetic order. */
-template <int NFIX>
+template <int NFIX, int REC>
 __device__ __forceinline__ int coupled_rhs_regsym(const Sys<1>& S, const DeviceProblem& P, double T,
                                                   double (&Xs)[1][UD], double (&F)[1][UD], double (&ua)[1][NUAa],
                                                   int (&iua)[1][NIUAa], const double (&ra)[1], const double (&cb)[1],
@@ -907,65 +1024,40 @@ __device__ __forceinline__ int coupled_rhs_regsym(const Sys<1>& S, const DeviceP
         const double ax = fma(rd, asum, xu);
         r = b - ax;
     }
-    double rt = r, x = xu, p = 0.0, pt = 0.0;
-    double prod[1] = {r * rt};
-    double rho1 = warp_tree_sum<1>(prod);
-    double rho2 = 0.0;
-    int done = 0;
-    bool exited = false;
-    for (int iter = 1; iter <= P.bicg_max_iter; iter++) {
-        if (iter == 1) {
-            p = r;
-            pt = rt;
-            if (fabs(rho1) < 1e-6) { exited = true; break; }
-        } else {
-            const double beta = rho1 / rho2;
-            p = fma(beta, p, r);
-            pt = fma(beta, pt, rt);
-        }
+    /* q = A v = v + v_f (G (u v)), q~ = A^T vt = vt + u (G (v_f vt)) with u = b X1sq, v_f = rD a */
+    auto apply = [&](const double (&v)[1], const double (&vt)[1], double (&qo)[1], double (&qto)[1]) {
         __syncwarp();
-        S.vp[i] = x1 * p;     /* z  = u p  */
-        S.vpt[i] = rd * pt;   /* z~ = v p~ */
+        S.vp[i] = x1 * v[0];     /* z  = u v  */
+        S.vpt[i] = rd * vt[0];   /* z~ = v_f vt */
         __syncwarp();
         double qs, qts;
         row_sums2(S.vp, S.vpt, qs, qts);
-        const double q = valid ? fma(rd, qs, p) : 0.0;
-        const double qt = valid ? fma(x1, qts, pt) : 0.0;
-        prod[0] = pt * q;
-        const double alpha = rho1 / warp_tree_sum<1>(prod);
-        x = fma(alpha, p, x);
-        r = fma(-alpha, q, r);
-        rt = fma(-alpha, qt, rt);
-        double ar[1] = {fabs(r)};
-        prod[0] = r * rt;
-        double rho_next;
-        const bool small = grp_sum_max_below<1, 1>(S, ar, prod, 1e-6, rho_next);
-        rho2 = rho1;
-        done++;
-        if (small) { exited = true; break; }
-        rho1 = rho_next;
-    }
-    if (!exited) capped = true;
+        qo[0] = valid ? fma(rd, qs, v[0]) : 0.0;
+        qto[0] = valid ? fma(x1, qts, vt[0]) : 0.0;
+    };
+    double rr[1] = {r}, xx[1] = {xu};
+    const int done = bicg_iterate<1, 1, REC>(S, P, rr, xx, apply, capped);
+    const double x = xx[0];
     F[0][IC] = x;
     return done;
 }
 
 /* the right-hand side a kernel variant uses */
-template <int U, int RHS, int G>
+template <int U, int RHS, int G, int REC>
 __device__ __forceinline__ int rhs_eval(const Sys<U, G>& S, const DeviceProblem& P, double T, double (&Xs)[U][UD],
                                         double (&F)[U][UD], double (&up)[U][NUPa], double (&ua)[U][NUAa],
                                         int (&iua)[U][NIUAa], const double (&ra)[U], const double (&cb)[U],
                                         const double (&grow)[32], bool& capped) {
     if constexpr (RHS == 0) {
-        return coupled_rhs<U, G>(S, P, T, Xs, F, up, ua, iua, capped);
+        return coupled_rhs<U, G, REC>(S, P, T, Xs, F, up, ua, iua, capped);
     } else if constexpr (RHS == 3 || RHS == 4) {
-        return coupled_rhs_sharedc<U, G, RHS == 4>(S, P, T, Xs, F, up, ua, iua, ra, cb, capped);
+        return coupled_rhs_sharedc<U, G, RHS == 4, REC>(S, P, T, Xs, F, up, ua, iua, ra, cb, capped);
     } else if constexpr (RHS == 5 || RHS == 6) {
         static_assert(U == 1 && G == 1, "the register-resident operator needs one unit per lane");
-        return coupled_rhs_regsym<RHS == 6 ? 32 : 0>(S, P, T, Xs, F, ua, iua, ra, cb, grow, capped);
+        return coupled_rhs_regsym<RHS == 6 ? 32 : 0, REC>(S, P, T, Xs, F, ua, iua, ra, cb, grow, capped);
     } else {
         static_assert(U == 1, "the register-resident operator needs one unit per lane");
-        return coupled_rhs_regw<RHS == 2 ? 32 : 0>(S, P, T, Xs, F, up, ua, iua, capped);
+        return coupled_rhs_regw<RHS == 2 ? 32 : 0, REC>(S, P, T, Xs, F, up, ua, iua, capped);
     }
 }
 
@@ -1014,7 +1106,7 @@ __constant__ double kRK4_A[4] = {0.0, 0.5, 0.5, 1.0};
  * The six stages run as one loop so the coupled right-hand side is inlined
  * once; stage s evaluates at X + dt * (sum_j<s a_sj K_j) with the terms
  * accumulated in the reference's order (first a product, then fmas). */
-template <int U, int RHS, int G>
+template <int U, int RHS, int G, int REC>
 __device__ __forceinline__ bool step_rkck45(const Sys<U, G>& S, const DeviceProblem& P, Lane<U>& L,
                                             double T, double dt, double (&Yn)[U][UD], double (&E)[U][UD],
                                             Counters& cnt, bool& capped) {
@@ -1048,7 +1140,7 @@ __device__ __forceinline__ bool step_rkck45(const Sys<U, G>& S, const DeviceProb
                     Xs[m][c] = fma(acc, dt, L.X[m][c]);
                 }
         }
-        cnt.bicg += rhs_eval<U, RHS, G>(S, P, Ts, Xs, F, L.up, L.ua, L.iua, L.ra, L.cb, L.grow, capped);
+        cnt.bicg += rhs_eval<U, RHS, G, REC>(S, P, Ts, Xs, F, L.up, L.ua, L.iua, L.ra, L.cb, L.grow, capped);
 #pragma unroll
         for (int j = 0; j < 6; j++)
 #pragma unroll
@@ -1081,7 +1173,7 @@ __device__ __forceinline__ bool step_rkck45(const Sys<U, G>& S, const DeviceProb
 
 /* classical RK4 step (the reference has only its fixed-step controller,
  * ErrorControllers.cuh:424-450) */
-template <int U, int RHS, int G>
+template <int U, int RHS, int G, int REC>
 __device__ __forceinline__ bool step_rk4(const Sys<U, G>& S, const DeviceProblem& P, Lane<U>& L,
                                          double T, double dt, double (&Yn)[U][UD], Counters& cnt, bool& capped) {
     double K[4][U][UD];
@@ -1115,7 +1207,7 @@ __device__ __forceinline__ bool step_rk4(const Sys<U, G>& S, const DeviceProblem
                     Xs[m][c] = st == 3 ? fma(kprev, dt, L.X[m][c]) : fma(kprev * kRK4_A[st], dt, L.X[m][c]);
                 }
         }
-        cnt.bicg += rhs_eval<U, RHS, G>(S, P, Ts, Xs, F, L.up, L.ua, L.iua, L.ra, L.cb, L.grow, capped);
+        cnt.bicg += rhs_eval<U, RHS, G, REC>(S, P, Ts, Xs, F, L.up, L.ua, L.iua, L.ra, L.cb, L.grow, capped);
 #pragma unroll
         for (int j = 0; j < 4; j++)
 #pragma unroll
@@ -1167,7 +1259,7 @@ __device__ __forceinline__ void store_dense(const Sys<U, G>& S, const DeviceProb
 
 /* ---------------------------------------------------------------------------
  * One reference Solve() of one system (Solver.cuh:82-648). */
-template <int U, int RHS, int G>
+template <int U, int RHS, int G, int REC>
 __device__ void run_period(const Sys<U, G>& S, const DeviceProblem& P, Lane<U>& L, Counters& cnt,
                            double (&TD)[2], double& T, int& do_idx) {
     const double TD1 = TD[1];
@@ -1234,7 +1326,7 @@ __device__ void run_period(const Sys<U, G>& S, const DeviceProblem& P, Lane<U>& 
         double Yn[U][UD], E[U][UD];
         bool finite;
         if (P.algorithm == 1) {
-            finite = step_rkck45<U, RHS, G>(S, P, L, T, dt, Yn, E, cnt, capped);
+            finite = step_rkck45<U, RHS, G, REC>(S, P, L, T, dt, Yn, E, cnt, capped);
             /* ErrorController_RKCK45 (ErrorControllers.cuh:454-542) */
             double rr = 1e30;
             int ru = 1;
@@ -1268,7 +1360,7 @@ __device__ void run_period(const Sys<U, G>& S, const DeviceProblem& P, Lane<U>& 
             newdt = fmin(newdt, P.dtmax);
             newdt = fmax(newdt, P.dtmin);
         } else {
-            finite = step_rk4<U, RHS, G>(S, P, L, T, dt, Yn, cnt, capped);
+            finite = step_rk4<U, RHS, G, REC>(S, P, L, T, dt, Yn, cnt, capped);
             if (!finite) { cnt.status |= BES_STATUS_NONFINITE; terminate = true; update = 0; }
             newdt = P.dt0;
         }
@@ -1479,7 +1571,7 @@ __device__ __forceinline__ void analysis_period_end(const Sys<U, G>& S, const De
  * one unit per lane (U = 1) and
  * exchanges the group's values through shared memory and a named barrier per
  * system slot (barrier 0 is left to __syncthreads). */
-template <int U, int RHS, int G>
+template <int U, int RHS, int G, int REC>
 __global__ void __launch_bounds__(RHS == 3 || RHS == 4 || G > 1 ? 256 : 128, 1) bes_ensemble_kernel(DeviceProblem P) {
     static_assert(G == 1 || U == 1, "multi-warp systems run one unit per lane");
     static_assert(G == 1 || (RHS != 1 && RHS != 2 && RHS != 5 && RHS != 6),
@@ -1551,6 +1643,7 @@ __global__ void __launch_bounds__(RHS == 3 || RHS == 4 || G > 1 ? 256 : 128, 1) 
         }
         if (k >= P.n_active) break;
         const int sid = P.order ? P.order[k] : k;
+        if (sid < 0 || sid >= P.n_systems) continue;   /* an order slot left unfilled */
         S.sid = sid;
         S.N = P.units[sid];
         S.off = P.unit_offset[sid];
@@ -1616,7 +1709,7 @@ __global__ void __launch_bounds__(RHS == 3 || RHS == 4 || G > 1 ? 256 : 128, 1) 
                     for (int c = 0; c < NIUA; c++) L.iua[m][c] = v ? P.iuacc_reset[c] : 0;
                 }
             }
-            run_period<U, RHS, G>(S, P, L, cnt, TD, T, do_idx);
+            run_period<U, RHS, G, REC>(S, P, L, cnt, TD, T, do_idx);
             if (P.period_ref) analysis_period_end<U, G>(S, P, L, per);
         }
         /* write-back (Solver.cuh:599-648) */

@@ -1,67 +1,9 @@
-/* bes_kernel_u2.cu -- solver kernel variants for systems of up to 64 units (2 units per lane, one warp). */
-#include "bes_kernel.cuh"
-#include "bes_launch.h"
+/* bes_kernel_u2.cu -- solver kernel variants for systems of up to 64 units
+ * on one warp (two units per lane), the reference's BiCG recurrence. */
+#include "bes_kernel_inst.cuh"
 
 namespace bes {
-
-template <>
-size_t cta_smem_t<2, 0, 1>(int warps) { return (size_t)(warps / 1) * WarpSmem<2, 1>::BYTES; }
-
-template <>
-cudaError_t occupancy_t<2, 0, 1>(int warps, int* ctas_per_sm) {
-    const size_t smem = cta_smem_t<2, 0, 1>(warps);
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(bes_ensemble_kernel<2, 0, 1>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, bes_ensemble_kernel<2, 0, 1>, 32 * warps, smem);
-}
-
-template <>
-cudaError_t launch_t<2, 0, 1>(const DeviceProblem& P, int grid, int warps, cudaStream_t stream) {
-    bes_ensemble_kernel<2, 0, 1><<<grid, 32 * warps, cta_smem_t<2, 0, 1>(warps), stream>>>(P);
-    return cudaGetLastError();
-}
-
-template <>
-size_t cta_smem_t<2, 3, 1>(int warps) { return (size_t)SharedCSmem<2, 1>::C_BYTES + (size_t)(warps / 1) * SharedCSmem<2, 1>::WARP_BYTES; }
-
-template <>
-cudaError_t occupancy_t<2, 3, 1>(int warps, int* ctas_per_sm) {
-    const size_t smem = cta_smem_t<2, 3, 1>(warps);
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(bes_ensemble_kernel<2, 3, 1>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, bes_ensemble_kernel<2, 3, 1>, 32 * warps, smem);
-}
-
-template <>
-cudaError_t launch_t<2, 3, 1>(const DeviceProblem& P, int grid, int warps, cudaStream_t stream) {
-    bes_ensemble_kernel<2, 3, 1><<<grid, 32 * warps, cta_smem_t<2, 3, 1>(warps), stream>>>(P);
-    return cudaGetLastError();
-}
-
-template <>
-size_t cta_smem_t<2, 4, 1>(int warps) { return (size_t)SharedCSmem<2, 1>::C_BYTES + (size_t)(warps / 1) * SharedCSmem<2, 1>::WARP_BYTES; }
-
-template <>
-cudaError_t occupancy_t<2, 4, 1>(int warps, int* ctas_per_sm) {
-    const size_t smem = cta_smem_t<2, 4, 1>(warps);
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(bes_ensemble_kernel<2, 4, 1>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, bes_ensemble_kernel<2, 4, 1>, 32 * warps, smem);
-}
-
-template <>
-cudaError_t launch_t<2, 4, 1>(const DeviceProblem& P, int grid, int warps, cudaStream_t stream) {
-    bes_ensemble_kernel<2, 4, 1><<<grid, 32 * warps, cta_smem_t<2, 4, 1>(warps), stream>>>(P);
-    return cudaGetLastError();
-}
-
+BES_KERNEL_VARIANT(2, 0, 1, 0, BES_SMEM_WARP(2, 1))
+BES_KERNEL_VARIANT(2, 3, 1, 0, BES_SMEM_SHARED(2, 1))
+BES_KERNEL_VARIANT(2, 4, 1, 0, BES_SMEM_SHARED(2, 1))
 }  // namespace bes

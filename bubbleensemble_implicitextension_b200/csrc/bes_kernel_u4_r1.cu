@@ -1,0 +1,9 @@
+/* bes_kernel_u4_r1.cu -- solver kernel variants for systems of up to 128 units
+ * on one warp (four units per lane), the single-reduction BiCG recurrence. */
+#include "bes_kernel_inst.cuh"
+
+namespace bes {
+BES_KERNEL_VARIANT(4, 0, 1, 1, BES_SMEM_WARP(4, 1))
+BES_KERNEL_VARIANT(4, 3, 1, 1, BES_SMEM_SHARED(4, 1))
+BES_KERNEL_VARIANT(4, 4, 1, 1, BES_SMEM_SHARED(4, 1))
+}  // namespace bes

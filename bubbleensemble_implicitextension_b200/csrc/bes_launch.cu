@@ -8,34 +8,41 @@ namespace bes {
 
 namespace {
 
-template <int U_, int RHS_, int G_>
+template <int U_, int RHS_, int G_, int REC_>
 struct Tag {
-    static constexpr int U = U_, RHS = RHS_, G = G_;
+    static constexpr int U = U_, RHS = RHS_, G = G_, REC = REC_;
 };
 
-/* calls f(Tag<U, RHS, G>{}) for the built variant v; false if v is not built */
-template <class F>
-bool dispatch(Variant v, F&& f) {
+template <int REC, class F>
+bool dispatch_rec(Variant v, F&& f) {
     const int key = v.U * 100 + v.rhs * 10 + v.G;
     switch (key) {
-        case 111: f(Tag<1, 1, 1>{}); return true;
-        case 121: f(Tag<1, 2, 1>{}); return true;
-        case 151: f(Tag<1, 5, 1>{}); return true;
-        case 161: f(Tag<1, 6, 1>{}); return true;
-        case 201: f(Tag<2, 0, 1>{}); return true;
-        case 231: f(Tag<2, 3, 1>{}); return true;
-        case 401: f(Tag<4, 0, 1>{}); return true;
-        case 431: f(Tag<4, 3, 1>{}); return true;
-        case 241: f(Tag<2, 4, 1>{}); return true;
-        case 441: f(Tag<4, 4, 1>{}); return true;
-        case 142: f(Tag<1, 4, 2>{}); return true;
-        case 144: f(Tag<1, 4, 4>{}); return true;
-        case 102: f(Tag<1, 0, 2>{}); return true;
-        case 132: f(Tag<1, 3, 2>{}); return true;
-        case 104: f(Tag<1, 0, 4>{}); return true;
-        case 134: f(Tag<1, 3, 4>{}); return true;
+        case 111: f(Tag<1, 1, 1, REC>{}); return true;
+        case 121: f(Tag<1, 2, 1, REC>{}); return true;
+        case 151: f(Tag<1, 5, 1, REC>{}); return true;
+        case 161: f(Tag<1, 6, 1, REC>{}); return true;
+        case 201: f(Tag<2, 0, 1, REC>{}); return true;
+        case 231: f(Tag<2, 3, 1, REC>{}); return true;
+        case 401: f(Tag<4, 0, 1, REC>{}); return true;
+        case 431: f(Tag<4, 3, 1, REC>{}); return true;
+        case 241: f(Tag<2, 4, 1, REC>{}); return true;
+        case 441: f(Tag<4, 4, 1, REC>{}); return true;
+        case 142: f(Tag<1, 4, 2, REC>{}); return true;
+        case 144: f(Tag<1, 4, 4, REC>{}); return true;
+        case 102: f(Tag<1, 0, 2, REC>{}); return true;
+        case 132: f(Tag<1, 3, 2, REC>{}); return true;
+        case 104: f(Tag<1, 0, 4, REC>{}); return true;
+        case 134: f(Tag<1, 3, 4, REC>{}); return true;
         default: return false;
     }
+}
+
+/* calls f(Tag<U, RHS, G, REC>{}) for the built variant v; false if v is not built */
+template <class F>
+bool dispatch(Variant v, F&& f) {
+    if (v.rec == 0) return dispatch_rec<0>(v, f);
+    if (v.rec == 1) return dispatch_rec<1>(v, f);
+    return false;
 }
 
 }  // namespace
@@ -46,7 +53,7 @@ bool variant_exists(Variant v) {
 
 size_t cta_smem_bytes(Variant v, int warps) {
     size_t r = 0;
-    dispatch(v, [&](auto t) { using T = decltype(t); r = cta_smem_t<T::U, T::RHS, T::G>(warps); });
+    dispatch(v, [&](auto t) { using T = decltype(t); r = cta_smem_t<T::U, T::RHS, T::G, T::REC>(warps); });
     return r;
 }
 
@@ -60,13 +67,13 @@ int max_warps_per_block(Variant v) {
 
 cudaError_t occupancy(Variant v, int warps, int* ctas_per_sm) {
     cudaError_t e = cudaErrorInvalidValue;
-    dispatch(v, [&](auto t) { using T = decltype(t); e = occupancy_t<T::U, T::RHS, T::G>(warps, ctas_per_sm); });
+    dispatch(v, [&](auto t) { using T = decltype(t); e = occupancy_t<T::U, T::RHS, T::G, T::REC>(warps, ctas_per_sm); });
     return e;
 }
 
 cudaError_t launch(Variant v, const DeviceProblem& P, int grid, int warps, cudaStream_t stream) {
     cudaError_t e = cudaErrorInvalidValue;
-    dispatch(v, [&](auto t) { using T = decltype(t); e = launch_t<T::U, T::RHS, T::G>(P, grid, warps, stream); });
+    dispatch(v, [&](auto t) { using T = decltype(t); e = launch_t<T::U, T::RHS, T::G, T::REC>(P, grid, warps, stream); });
     return e;
 }
 
@@ -75,15 +82,15 @@ cudaError_t launch(Variant v, const DeviceProblem& P, int grid, int warps, cudaS
  * on 2 or 4 warps (or 2 or 4 units per lane on one warp) with W in shared
  * memory, or one staged copy of a matrix shared by the whole class when the
  * caller asked for shared coupling matrices (SharedCouplingMatrices). */
-Variant class_variant(int cls, bool all32, bool shared, int warps_per_system, bool symmetric) {
+Variant class_variant(int cls, bool all32, bool shared, int warps_per_system, bool symmetric, int rec) {
     if (cls == 0) {
-        if (shared && symmetric) return Variant{1, all32 ? 6 : 5, 1};   /* row of G in registers */
-        return Variant{1, all32 ? 2 : 1, 1};
+        if (shared && symmetric) return Variant{1, all32 ? 6 : 5, 1, rec};   /* row of G in registers */
+        return Variant{1, all32 ? 2 : 1, 1, rec};
     }
     const int rhs = shared ? (symmetric ? 4 : 3) : 0;
     const int width = cls == 1 ? 2 : 4;
-    if (warps_per_system == 1) return Variant{width, rhs, 1};
-    return Variant{1, rhs, width};
+    if (warps_per_system == 1) return Variant{width, rhs, 1, rec};
+    return Variant{1, rhs, width, rec};
 }
 
 /* CTA shape of a launch of `count` systems: spread small ensembles over every

@@ -9,7 +9,8 @@
  * per CTA (64 or 128 units), RHS 4 is RHS 3 for a symmetric shared matrix
  * (both BiCG products as row sums from one shared-memory read); RHS 5 / 6
  * (U = G = 1, N <= 32) keep a row of a shared symmetric matrix in registers
- * (6: every system has 32 units). */
+ * (6: every system has 32 units).  Every variant exists with both BiCG
+ * recurrences (REC 0: the reference's; 1: the single-reduction form). */
 #ifndef BES_LAUNCH_H
 #define BES_LAUNCH_H
 
@@ -20,9 +21,11 @@
 
 namespace bes {
 
-/* a kernel variant */
+/* a kernel variant; rec selects the BiCG recurrence (0: the reference's,
+ * 1: the single-reduction form) */
 struct Variant {
     int U, rhs, G;
+    int rec = 0;
 };
 
 /* is (U, RHS, G) one of the built variants */
@@ -38,17 +41,18 @@ cudaError_t launch(Variant v, const DeviceProblem& P, int grid, int warps, cudaS
 
 /* variant of units class cls (0: N <= 32, 1: N <= 64, 2: N <= 128); all32:
  * every system of the launch has 32 units; shared: the launch shares one
- * coupling matrix; warps_per_system 1 keeps every system on one warp */
-Variant class_variant(int cls, bool all32, bool shared, int warps_per_system, bool symmetric = false);
+ * coupling matrix; warps_per_system 1 keeps every system on one warp; rec:
+ * the BiCG recurrence */
+Variant class_variant(int cls, bool all32, bool shared, int warps_per_system, bool symmetric = false, int rec = 0);
 /* warps per CTA for `count` systems of variant v (requested > 0: that many,
  * clamped to what the variant allows and rounded down to a multiple of G) */
 int class_warps_per_block(Variant v, int count, int sm_count, int requested);
 
-template <int U, int RHS, int G>
+template <int U, int RHS, int G, int REC>
 size_t cta_smem_t(int warps);
-template <int U, int RHS, int G>
+template <int U, int RHS, int G, int REC>
 cudaError_t occupancy_t(int warps, int* ctas_per_sm);
-template <int U, int RHS, int G>
+template <int U, int RHS, int G, int REC>
 cudaError_t launch_t(const DeviceProblem& P, int grid, int warps, cudaStream_t stream);
 
 }  // namespace bes

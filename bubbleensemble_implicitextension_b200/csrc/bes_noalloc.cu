@@ -52,11 +52,17 @@ cudaError_t g_scratch_err[BES_NOALLOC_MAX_DEVICES] = {};
 int units_class(int n) { return n <= 32 ? 0 : (n <= 64 ? 1 : 2); }
 
 /* Zero the counters and write each class's systems, in index order, into its
- * segment of the order: warp c handles class c, 32 systems per ballot. */
+ * segment of the order: warp c handles class c, 32 systems per ballot.  The
+ * order is first filled with -1, which the solver kernel skips: if the device
+ * unit counts disagree with the host copy the plan was made from, a class
+ * segment may be left partly unwritten, and no stale index from an earlier
+ * call survives in it. */
 __global__ void noalloc_prepare(const int32_t* __restrict__ units, int n, int32_t* scratch, int begin0, int begin1,
                                 int begin2) {
     const int lane = threadIdx.x & 31, cls = threadIdx.x >> 5;
     if (threadIdx.x < 4) scratch[threadIdx.x] = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) scratch[4 + i] = -1;
+    __syncthreads();
     if (cls > 2) return;
     int pos = 4 + (cls == 0 ? begin0 : (cls == 1 ? begin1 : begin2));
     for (int base = 0; base < n; base += 32) {
@@ -97,6 +103,9 @@ extern "C" bes_status bes_solve_periods_noalloc(const bes_noalloc_problem* p, in
         return report(p, BES_ERR_ARGUMENT, "bes_solve_periods_noalloc: a required array pointer is null", 0, 0);
     if (p->algorithm != BES_RK4 && p->algorithm != BES_RKCK45)
         return report(p, BES_ERR_ARGUMENT, "bes_solve_periods_noalloc: unknown algorithm %lld", (long long)p->algorithm, 0);
+    if (p->bicg_recurrence != 0 && p->bicg_recurrence != 1)
+        return report(p, BES_ERR_ARGUMENT, "bes_solve_periods_noalloc: bicg_recurrence %lld is not 0 or 1",
+                      (long long)p->bicg_recurrence, 0);
 
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= BES_NOALLOC_MAX_DEVICES)
@@ -122,9 +131,50 @@ extern "C" bes_status bes_solve_periods_noalloc(const bes_noalloc_problem* p, in
         if (units_class(n) == 0 && n != 32) all32 = false;
     }
     const int begin[3] = {0, count[0], count[0] + count[1]};
+    /* options: 0 takes the SolverOption default (Interface.cuh:613-618), a negative value is an error */
+    const double opt[5] = {p->dt0, p->dtmin, p->dtmax, p->grow, p->shrink};
+    const double dflt[5] = {1e-2, 1e-12, 1e6, 5.0, 0.1};
+    const char* opt_name[5] = {"dt0", "dtmin", "dtmax", "grow", "shrink"};
+    double val[5];
+    for (int k = 0; k < 5; k++) {
+        if (!(opt[k] >= 0.0)) {
+            if (p->error_message && p->error_capacity > 0)
+                std::snprintf(p->error_message, (size_t)p->error_capacity,
+                              "bes_solve_periods_noalloc: option %s = %g is negative or not a number", opt_name[k], opt[k]);
+            return BES_ERR_ARGUMENT;
+        }
+        val[k] = opt[k] == 0.0 ? dflt[k] : opt[k];
+    }
+    /* the launch shapes, checked before anything is queued */
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
+    bes::Variant var[3];
+    int wpb[3] = {0, 0, 0}, grid[3] = {0, 0, 0};
+    cudaError_t e = cudaSuccess;
+    for (int cls = 0; cls < 3; cls++) {
+        if (count[cls] == 0) continue;
+        var[cls] = bes::class_variant(cls, all32, false, 0, false, p->bicg_recurrence);
+        const bes::Variant& v = var[cls];
+        if (bes::max_warps_per_block(v) < v.G)
+            return report(p, BES_ERR_CUDA, "bes_solve_periods_noalloc: kernel class %lld (%lld warps per system) does not fit in shared memory",
+                          (long long)cls, (long long)v.G);
+        wpb[cls] = bes::class_warps_per_block(v, count[cls], sms, p->warps_per_block);
+        int per_sm = 0;
+        e = bes::occupancy(v, wpb[cls], &per_sm);
+        if (e != cudaSuccess || per_sm < 1)
+            return report(p, BES_ERR_CUDA, "bes_solve_periods_noalloc: kernel class %lld cannot be resident (cudaError %lld)",
+                          (long long)cls, (long long)e);
+        const int needed = (count[cls] + wpb[cls] / v.G - 1) / (wpb[cls] / v.G);
+        grid[cls] = needed < per_sm * sms ? needed : per_sm * sms;
+    }
     cudaStream_t st = (cudaStream_t)stream;
+    /* an error left pending by the caller's earlier work is reported as such (and not cleared) */
+    e = cudaPeekAtLastError();
+    if (e != cudaSuccess)
+        return report(p, BES_ERR_CUDA, "bes_solve_periods_noalloc: a CUDA error from earlier work is pending (cudaError %lld)",
+                      (long long)e, 0);
     noalloc_prepare<<<1, 96, 0, st>>>(p->units, p->n_systems, scratch, begin[0], begin[1], begin[2]);
-    cudaError_t e = cudaGetLastError();
+    e = cudaGetLastError();
     if (e != cudaSuccess)
         return report(p, BES_ERR_CUDA, "bes_solve_periods_noalloc: prepare launch failed (cudaError %lld)", (long long)e, 0);
 
@@ -150,11 +200,11 @@ extern "C" bes_status bes_solve_periods_noalloc(const bes_noalloc_problem* p, in
     P.atol = p->atol;
     P.event_tol = p->event_tol;
     P.event_dir = p->event_dir;
-    P.dt0 = p->dt0;
-    P.dtmin = p->dtmin;
-    P.dtmax = p->dtmax;
-    P.grow = p->grow;
-    P.shrink = p->shrink;
+    P.dt0 = val[0];
+    P.dtmin = val[1];
+    P.dtmax = val[2];
+    P.grow = val[3];
+    P.shrink = val[4];
     P.algorithm = p->algorithm;
     P.bicg_max_iter = p->bicg_max_iter > 0 ? p->bicg_max_iter : 19;
     P.max_steps_per_period = p->max_steps_per_period > 0 ? p->max_steps_per_period : 1000000;
@@ -174,23 +224,12 @@ extern "C" bes_status bes_solve_periods_noalloc(const bes_noalloc_problem* p, in
     P.uacc_reset = p->uacc_reset;
     P.iuacc_reset = p->iuacc_reset;
 
-    int sms = 0;
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
     for (int cls = 0; cls < 3; cls++) {
         if (count[cls] == 0) continue;
-        const bes::Variant v = bes::class_variant(cls, all32, false, 0);
         P.order = scratch + 4 + begin[cls];
         P.n_active = count[cls];
         P.work_counter = scratch + cls;
-        const int wpb = bes::class_warps_per_block(v, count[cls], sms, p->warps_per_block);
-        int per_sm = 0;
-        e = bes::occupancy(v, wpb, &per_sm);
-        if (e != cudaSuccess || per_sm < 1)
-            return report(p, BES_ERR_CUDA, "bes_solve_periods_noalloc: kernel class %lld cannot be resident (cudaError %lld)",
-                          (long long)cls, (long long)e);
-        const int needed = (count[cls] + wpb / v.G - 1) / (wpb / v.G);
-        const int grid = needed < per_sm * sms ? needed : per_sm * sms;
-        e = bes::launch(v, P, grid, wpb, st);
+        e = bes::launch(var[cls], P, grid[cls], wpb[cls], st);
         if (e != cudaSuccess)
             return report(p, BES_ERR_CUDA, "bes_solve_periods_noalloc: launch of class %lld failed (cudaError %lld)",
                           (long long)cls, (long long)e);

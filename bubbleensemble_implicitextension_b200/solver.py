@@ -75,6 +75,7 @@ class ListOfSolverOptions(IntEnum):
     WarpsPerBlock = 102
     UseCudaGraph = 103
     WarpsPerSystem = 104
+    BiCGRecurrence = 105
 
 
 class Algorithms(IntEnum):
@@ -182,7 +183,7 @@ class NoallocProblem(ctypes.Structure):
         ("ndo", ctypes.c_int32), ("do_save_frequency", ctypes.c_int32),
         ("bicg_max_iter", ctypes.c_int32), ("warps_per_block", ctypes.c_int32),
         ("max_steps_per_period", ctypes.c_int64),
-        ("error_message", ctypes.c_char_p), ("error_capacity", ctypes.c_int32), ("pad", ctypes.c_int32),
+        ("error_message", ctypes.c_char_p), ("error_capacity", ctypes.c_int32), ("bicg_recurrence", ctypes.c_int32),
     ]
 
 

@@ -102,6 +102,12 @@ typedef int32_t bes_status;
 #define BES_OPT_WARPS_PER_SYSTEM 104       /* 0 (default): systems of 33-64 units run on 2 warps and of 65-128
                                               units on 4 warps (one unit per lane); 1: one warp per system
                                               (2 or 4 units per lane).  Results are bit-identical. */
+#define BES_OPT_BICG_RECURRENCE 105        /* 0 (default): the reference's BiCG recurrence (Steppers.cuh:508-561:
+                                              two reductions per iteration); 1: the single-reduction form of the
+                                              same iterates (residual products first, rho = r.r~ and mu = r~.Ar
+                                              in one reduction, sigma = mu - beta^2 sigma_prev).  Equal in exact
+                                              arithmetic, rounded differently: results stay within the parity
+                                              tolerances of the reference, not bit-identical to option 0. */
 
 /* Algorithms, Interface.cuh:33 */
 #define BES_RK4 0
@@ -337,7 +343,9 @@ typedef struct bes_noalloc_problem {
     int32_t n_systems;
     int32_t algorithm;                 /* BES_RK4 or BES_RKCK45 */
     int64_t total_units;
-    const int32_t* units_host;         /* host copy of the unit counts [n_systems] (launch planning) */
+    const int32_t* units_host;         /* host copy of the unit counts [n_systems] (launch planning); must
+                                          hold the same values as the device array `units` (a system whose
+                                          class disagrees may be skipped, never read out of bounds) */
     /* device arrays */
     const int32_t* units;              /* [n_systems] */
     const int64_t* unit_offset;        /* [n_systems] */
@@ -368,14 +376,17 @@ typedef struct bes_noalloc_problem {
     uint64_t* n_bicg_iter;
     uint64_t* n_rhs;
     int32_t* status;                   /* [n_systems], OR of BES_STATUS_* */
-    /* options (defaults of SolverOption where 0) */
+    /* options: a field left 0 takes the default of SolverOption (Interface.cuh:613-618):
+     * dt0 1e-2, dtmin 1e-12, dtmax 1e6, grow 5, shrink 0.1, bicg_max_iter 19,
+     * max_steps_per_period 1e6, do_save_frequency 1 (do_min_dt and ndo: 0);
+     * a negative dt0, dtmin, dtmax, grow or shrink is rejected with BES_ERR_ARGUMENT */
     double dt0, dtmin, dtmax, grow, shrink, do_min_dt;
     int32_t ndo, do_save_frequency;
     int32_t bicg_max_iter, warps_per_block;
     int64_t max_steps_per_period;
     char* error_message;               /* optional caller buffer for a message on failure */
     int32_t error_capacity;
-    int32_t pad;
+    int32_t bicg_recurrence;           /* BES_OPT_BICG_RECURRENCE: 0 (reference) or 1 */
 } bes_noalloc_problem;
 bes_status bes_solve_periods_noalloc(const bes_noalloc_problem* problem, int32_t n_periods, int32_t reset_at,
                                      void* stream);

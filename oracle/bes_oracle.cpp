@@ -117,12 +117,13 @@ inline double tree_max(const double* v, int n, double* tmp) {
 
 struct Work {
     int N;
-    std::vector<double> cpt, rd, x1sq, xu, b, r, rt, p, pt, q, qt, x, W, tmp, tmp2, us, vs;
+    std::vector<double> cpt, rd, x1sq, xu, b, r, rt, p, pt, q, qt, x, W, tmp, tmp2, us, vs, z, zt, wv, wtv;
     explicit Work(int n) : N(n) {
         int P = next_pow2_32(n);
         cpt.resize(n); rd.resize(n); x1sq.resize(n); xu.resize(n); b.resize(n);
         r.resize(n); rt.resize(n); p.resize(n); pt.resize(n); q.resize(n); qt.resize(n);
         x.resize(n); W.resize((size_t)n * n); tmp.resize(P); tmp2.resize(n); us.resize(n); vs.resize(n);
+        z.resize(n); zt.resize(n); wv.resize(n); wtv.resize(n);
     }
 };
 
@@ -135,7 +136,7 @@ struct Work {
 int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
                 const double* up, long ups, const double* C, int max_iter,
                 double* f0, double* f1, bool* capped, bool shared_assoc = false,
-                const double* ra = nullptr, const double* cb = nullptr, bool symmetric = false) {
+                const double* ra = nullptr, const double* cb = nullptr, bool symmetric = false, int variant = 0) {
     const int N = w.N;
     double upl[NUP];
     for (int i = 0; i < N; i++) {
@@ -170,59 +171,112 @@ int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
         w.x[i] = w.xu[i];
         for (int j = 0; j < N; j++) w.W[i + (long)j * N] = (w.rd[i] * C[i + (long)j * N]) * w.x1sq[j];
     }
-    for (int i = 0; i < N; i++) w.tmp2[i] = w.r[i] * w.rt[i];
-    double rho1 = tree_sum(w.tmp2.data(), N, w.tmp.data());
-    double rho2 = 0.0;
-    int done = 0;
-    bool exited = false;
-    for (int iter = 1; iter <= max_iter; iter++) {
-        if (iter == 1) {
-            for (int i = 0; i < N; i++) { w.p[i] = w.r[i]; w.pt[i] = w.rt[i]; }
-            if (std::fabs(rho1) < 1e-6) { exited = true; break; }
-        } else {
-            double beta = rho1 / rho2;
-            for (int i = 0; i < N; i++) {
-                w.p[i] = fma(beta, w.p[i], w.r[i]);
-                w.pt[i] = fma(beta, w.pt[i], w.rt[i]);
-            }
-        }
-        /* q = A p (row sums) and qt = A^T pt (tree sums), Steppers.cuh:669-706 */
+    /* q = A v (row sums) and qt = A^T vt (tree sums or, for a symmetric shared
+     * matrix, row sums), Steppers.cuh:669-706 */
+    auto apply = [&](const double* v, const double* vt, double* q, double* qt) {
         if (shared_assoc) {
-            for (int j = 0; j < N; j++) { w.b[j] = w.us[j] * w.p[j]; w.xu[j] = w.vs[j] * w.pt[j]; }
-            /* w.b, w.xu reused as the scaled vectors z = u p and z~ = v p~ (x_u is no longer needed) */
+            for (int j = 0; j < N; j++) { w.z[j] = w.us[j] * v[j]; w.zt[j] = w.vs[j] * vt[j]; }
         }
         for (int i = 0; i < N; i++) {
             if (shared_assoc) {
-                double s = row_sum4(N, [&](int j) { return C[i + (long)j * N]; }, [&](int j) { return w.b[j]; });
-                w.q[i] = fma(w.vs[i], s, w.p[i]);
+                double s = row_sum4(N, [&](int j) { return C[i + (long)j * N]; }, [&](int j) { return w.z[j]; });
+                q[i] = fma(w.vs[i], s, v[i]);
                 if (symmetric) {
                     /* C = C^T: the transposed product as a row sum (the kernel reads each entry once for both) */
-                    double st = row_sum4(N, [&](int j) { return C[i + (long)j * N]; }, [&](int j) { return w.xu[j]; });
-                    w.qt[i] = fma(w.us[i], st, w.pt[i]);
+                    double st = row_sum4(N, [&](int j) { return C[i + (long)j * N]; }, [&](int j) { return w.zt[j]; });
+                    qt[i] = fma(w.us[i], st, vt[i]);
                 } else {
-                    for (int j = 0; j < N; j++) w.tmp2[j] = C[j + (long)i * N] * w.xu[j];
-                    w.qt[i] = fma(w.us[i], tree_sum(w.tmp2.data(), N, w.tmp.data()), w.pt[i]);
+                    for (int j = 0; j < N; j++) w.tmp2[j] = C[j + (long)i * N] * w.zt[j];
+                    qt[i] = fma(w.us[i], tree_sum(w.tmp2.data(), N, w.tmp.data()), vt[i]);
                 }
             } else {
-                w.q[i] = w.p[i] + row_sum4(N, [&](int j) { return w.W[i + (long)j * N]; }, [&](int j) { return w.p[j]; });
-                for (int j = 0; j < N; j++) w.tmp2[j] = w.W[j + (long)i * N] * w.pt[j];
-                w.qt[i] = w.pt[i] + tree_sum(w.tmp2.data(), N, w.tmp.data());
+                q[i] = v[i] + row_sum4(N, [&](int j) { return w.W[i + (long)j * N]; }, [&](int j) { return v[j]; });
+                for (int j = 0; j < N; j++) w.tmp2[j] = w.W[j + (long)i * N] * vt[j];
+                qt[i] = vt[i] + tree_sum(w.tmp2.data(), N, w.tmp.data());
             }
         }
-        for (int i = 0; i < N; i++) w.tmp2[i] = w.pt[i] * w.q[i];
-        double alpha = rho1 / tree_sum(w.tmp2.data(), N, w.tmp.data());
-        for (int i = 0; i < N; i++) {
-            w.x[i] = fma(alpha, w.p[i], w.x[i]);
-            w.r[i] = fma(-alpha, w.q[i], w.r[i]);
-            w.rt[i] = fma(-alpha, w.qt[i], w.rt[i]);
-        }
-        for (int i = 0; i < N; i++) w.tmp2[i] = std::fabs(w.r[i]);
-        double rmax = tree_max(w.tmp2.data(), N, w.tmp.data());
-        rho2 = rho1;
-        done++;
-        if (rmax < 1e-6) { exited = true; break; }
+    };
+    int done = 0;
+    bool exited = false;
+    if (variant == 0) {
+        /* the reference's recurrence, Steppers.cuh:508-561 */
         for (int i = 0; i < N; i++) w.tmp2[i] = w.r[i] * w.rt[i];
-        rho1 = tree_sum(w.tmp2.data(), N, w.tmp.data());
+        double rho1 = tree_sum(w.tmp2.data(), N, w.tmp.data());
+        double rho2 = 0.0;
+        for (int iter = 1; iter <= max_iter; iter++) {
+            if (iter == 1) {
+                for (int i = 0; i < N; i++) { w.p[i] = w.r[i]; w.pt[i] = w.rt[i]; }
+                if (std::fabs(rho1) < 1e-6) { exited = true; break; }
+            } else {
+                double beta = rho1 / rho2;
+                for (int i = 0; i < N; i++) {
+                    w.p[i] = fma(beta, w.p[i], w.r[i]);
+                    w.pt[i] = fma(beta, w.pt[i], w.rt[i]);
+                }
+            }
+            apply(w.p.data(), w.pt.data(), w.q.data(), w.qt.data());
+            for (int i = 0; i < N; i++) w.tmp2[i] = w.pt[i] * w.q[i];
+            double alpha = rho1 / tree_sum(w.tmp2.data(), N, w.tmp.data());
+            for (int i = 0; i < N; i++) {
+                w.x[i] = fma(alpha, w.p[i], w.x[i]);
+                w.r[i] = fma(-alpha, w.q[i], w.r[i]);
+                w.rt[i] = fma(-alpha, w.qt[i], w.rt[i]);
+            }
+            for (int i = 0; i < N; i++) w.tmp2[i] = std::fabs(w.r[i]);
+            double rmax = tree_max(w.tmp2.data(), N, w.tmp.data());
+            rho2 = rho1;
+            done++;
+            if (rmax < 1e-6) { exited = true; break; }
+            for (int i = 0; i < N; i++) w.tmp2[i] = w.r[i] * w.rt[i];
+            rho1 = tree_sum(w.tmp2.data(), N, w.tmp.data());
+        }
+    } else {
+        /* Single-reduction recurrence (the same iterates in exact arithmetic):
+         * the products of the residuals w = A r, w~ = A^T r~ come first, then
+         * one reduction gives rho = r.r~ and mu = r~.w together, and
+         *   beta = rho / rho_prev,  sigma = mu - beta^2 sigma_prev,
+         *   p = r + beta p, p~ = r~ + beta p~, q = w + beta q, q~ = w~ + beta q~,
+         *   alpha = rho / sigma,
+         * so that q = A p, q~ = A^T p~ and sigma = p~.A p (the two cross terms
+         * of p~.A p equal -rho/alpha_prev each by the biorthogonality of the
+         * residuals, and rho/alpha_prev = beta sigma_prev).  The exits are the
+         * reference's: |rho| < 1e-6 before the first update, max |r| < 1e-6
+         * after each update, at most max_iter updates. */
+        double sigma = 0.0, rho_prev = 0.0;
+        for (int iter = 1; iter <= max_iter; iter++) {
+            apply(w.r.data(), w.rt.data(), w.wv.data(), w.wtv.data());
+            for (int i = 0; i < N; i++) w.tmp2[i] = w.r[i] * w.rt[i];
+            const double rho = tree_sum(w.tmp2.data(), N, w.tmp.data());
+            for (int i = 0; i < N; i++) w.tmp2[i] = w.rt[i] * w.wv[i];
+            const double mu = tree_sum(w.tmp2.data(), N, w.tmp.data());
+            if (iter == 1) {
+                if (std::fabs(rho) < 1e-6) { exited = true; break; }
+                for (int i = 0; i < N; i++) {
+                    w.p[i] = w.r[i]; w.pt[i] = w.rt[i]; w.q[i] = w.wv[i]; w.qt[i] = w.wtv[i];
+                }
+                sigma = mu;
+            } else {
+                const double beta = rho / rho_prev;
+                sigma = fma(-(beta * beta), sigma, mu);
+                for (int i = 0; i < N; i++) {
+                    w.p[i] = fma(beta, w.p[i], w.r[i]);
+                    w.pt[i] = fma(beta, w.pt[i], w.rt[i]);
+                    w.q[i] = fma(beta, w.q[i], w.wv[i]);
+                    w.qt[i] = fma(beta, w.qt[i], w.wtv[i]);
+                }
+            }
+            const double alpha = rho / sigma;
+            rho_prev = rho;
+            for (int i = 0; i < N; i++) {
+                w.x[i] = fma(alpha, w.p[i], w.x[i]);
+                w.r[i] = fma(-alpha, w.q[i], w.r[i]);
+                w.rt[i] = fma(-alpha, w.qt[i], w.rt[i]);
+            }
+            for (int i = 0; i < N; i++) w.tmp2[i] = std::fabs(w.r[i]);
+            const double rmax = tree_max(w.tmp2.data(), N, w.tmp.data());
+            done++;
+            if (rmax < 1e-6) { exited = true; break; }
+        }
     }
     *capped = !exited;
     for (int i = 0; i < N; i++) f1[i] = w.x[i];
@@ -275,7 +329,8 @@ struct SystemRun {
         int it = coupled_rhs(w, T, a0, a1, up(), tot, C(), P->bicg_max_iter, f0, f1, &capped,
                              P->shared_assoc != 0 && (N > 32 || symmetric_C),
                              P->coupling_row_scale ? P->coupling_row_scale + off : nullptr,
-                             P->coupling_col_scale ? P->coupling_col_scale + off : nullptr, symmetric_C);
+                             P->coupling_col_scale ? P->coupling_col_scale + off : nullptr, symmetric_C,
+                             P->bicg_variant);
         nbicg += it;
         if (capped) capped_any = true;
         return it;
@@ -467,6 +522,7 @@ struct SystemRun {
                 break;
             }
             attempted++;
+            if (p->min_dt && dt < p->min_dt[s]) p->min_dt[s] = dt;
             bool capped = false;
             bool finite = p->algorithm == 1 ? step_rkck45(T, dt, p->n_bicg_iter[s], p->n_rhs[s], capped)
                                              : step_rk4(T, dt, p->n_bicg_iter[s], p->n_rhs[s], capped);

@@ -83,6 +83,13 @@ typedef struct bes_oracle_problem {
      * system s couples units i, j through a_i G_ij b_j, G its stored matrix */
     const double* coupling_row_scale;
     const double* coupling_col_scale;
+    /* 0: the reference's BiCG recurrence (two reductions per iteration);
+     * 1: the single-reduction recurrence (see coupled_rhs in the .cpp) */
+    int32_t bicg_variant;
+    int32_t pad;
+    /* optional [n_systems] output, or NULL: the smallest step size attempted
+     * (min over the periods of this call and the value already stored) */
+    double* min_dt;
 } bes_oracle_problem;
 
 /* Integrate `n_periods` reference Solve() calls for every active system.

@@ -1,7 +1,8 @@
 """TEST INFRASTRUCTURE: build recipe for the reference's own CUDA solver.
 
 Compiles oracle/ref_harness.cu against the reference's unmodified headers in
-place (``/root/reference`` and ``/root/reference/SourceCodes``) with the
+place (the reference tree and its ``SourceCodes`` directory, given as an
+argument or by the environment variable ``BES_REFERENCE_DIR``) with the
 reference's own nvcc flags (makefile:2), except ``sm_100a`` for ``sm_35``.
 Outputs go to ``oracle/_ref/`` only (git-ignored; the built binaries travel
 with the tree to the GPU machine, the reference sources do not).
@@ -19,7 +20,16 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-REFERENCE = Path(os.environ.get("BES_REFERENCE_DIR", "/root/reference"))
+MARKER = OUT / "reference_dir.txt"   # the tree the last build() used (git-ignored, like the binaries)
+
+
+def reference_dir(given=None):
+    """The reference tree: the argument, else $BES_REFERENCE_DIR, else the tree
+    the last build() used, else None."""
+    d = given or os.environ.get("BES_REFERENCE_DIR")
+    if not d and MARKER.exists():
+        d = MARKER.read_text().strip()
+    return Path(d) if d else None
 
 # (units per system, max systems, dense-output slots, register cap)
 VARIANTS = [
@@ -38,11 +48,12 @@ def path(ups: int, ns: int, ndo: int = 0, cap: bool = True) -> Path:
     return OUT / name(ups, ns, ndo, cap)
 
 
-def available() -> bool:
-    return (REFERENCE / "SourceCodes" / "CoupledSystems_PerBlock_Interface.cuh").exists()
+def available(reference=None) -> bool:
+    ref = reference_dir(reference)
+    return ref is not None and (ref / "SourceCodes" / "CoupledSystems_PerBlock_Interface.cuh").exists()
 
 
-def _one(v) -> Path:
+def _one(v, ref: Path) -> Path:
     ups, ns, ndo, cap = v
     exe = path(ups, ns, ndo, cap)
     src = HERE / "ref_harness.cu"
@@ -51,7 +62,7 @@ def _one(v) -> Path:
     nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
     cmd = [nvcc, "-O3", "--std=c++11", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-w",
            f"-DHARNESS_UPS={ups}", f"-DHARNESS_NS={ns}", f"-DHARNESS_NDO={ndo}",
-           "-I", str(REFERENCE), "-I", str(REFERENCE / "SourceCodes"), str(src), "-o", str(exe)]
+           "-I", str(ref), "-I", str(ref / "SourceCodes"), str(src), "-o", str(exe)]
     if cap:
         cmd.insert(1, "-maxrregcount=128")
     res = subprocess.run(cmd, capture_output=True, text=True)
@@ -93,15 +104,49 @@ def build_dropin() -> list[Path]:
     return outs
 
 
-def build() -> list[Path]:
-    """Build every variant (no-op when the reference tree is absent)."""
-    if not available():
+def build(reference=None) -> list[Path]:
+    """Build every variant from the reference tree `reference` (default
+    $BES_REFERENCE_DIR); a no-op when no reference tree is given or found."""
+    if not available(reference):
         return []
+    ref = reference_dir(reference)
     OUT.mkdir(exist_ok=True)
+    MARKER.write_text(str(ref) + "\n")
     with cf.ThreadPoolExecutor(max_workers=min(len(VARIANTS), os.cpu_count() or 1)) as ex:
-        return list(ex.map(_one, VARIANTS))
+        return list(ex.map(lambda v: _one(v, ref), VARIANTS))
+
+
+# the reference's own drivers and the -D flags they need (BubbleEnsemble.cu uses NCOLL,
+# which only CollapseStrength.cu defines)
+DRIVERS = {"CollapseStrength": [], "BubbleEnsemble": ["-DNCOLL=32"]}
+
+
+def build_reference_drivers(outdir: Path, reference=None) -> dict:
+    """Compile the reference's own driver programs, unchanged, against
+    include/dropin/ and link them with libbes.so (the drop-in: the drivers'
+    ProblemSolver<...> runs on this library).  Returns {driver: executable};
+    empty when no reference tree is found."""
+    ref = reference_dir(reference)
+    if ref is None or not (ref / "CollapseStrength.cu").exists():
+        return {}
+    root = HERE.parent
+    pkg = root / "bubbleensemble_implicitextension_b200"
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    outdir.mkdir(parents=True, exist_ok=True)
+    out = {}
+    for drv, flags in DRIVERS.items():
+        exe = outdir / f"dropin_{drv}"
+        cmd = [nvcc, "-O2", "--std=c++17", "-w", *flags, "-I", str(root / "include" / "dropin"),
+               "-I", str(root / "include"), str(ref / f"{drv}.cu"), "-o", str(exe),
+               "-L", str(pkg), "-lbes", "-Xlinker", f"-rpath={pkg}"]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"{drv}.cu does not build against the drop-in:\n{res.stderr[-4000:]}")
+        out[drv] = exe
+    return out
 
 
 if __name__ == "__main__":
-    for p in build():
+    import sys
+    for p in build(sys.argv[1] if len(sys.argv) > 1 else None):
         print(p)

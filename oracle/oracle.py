@@ -36,6 +36,7 @@ class Problem(ctypes.Structure):
         ("dense_time", _dp), ("dense_state", _dp), ("dense_index", _i32p),
         ("n_accepted", _i64p), ("n_rejected", _i64p), ("n_bicg_iter", _i64p), ("n_rhs", _i64p),
         ("status", _i32p), ("coupling_row_scale", _dp), ("coupling_col_scale", _dp),
+        ("bicg_variant", ctypes.c_int32), ("pad", ctypes.c_int32), ("min_dt", _dp),
     ]
 
 
@@ -80,7 +81,8 @@ def _p(a, t):
 
 def run(ens, n_periods: int = None, reset_at: int = None, threads: int = 0, systems=None,
         algorithm: int = 1, ndo: int = 0, do_min_dt: float = 0.0, do_save_frequency: int = 1,
-        bicg_max_iter: int = 19, uacc=None, iuacc=None, state=None, shared_assoc=None) -> dict:
+        bicg_max_iter: int = 19, uacc=None, iuacc=None, state=None, shared_assoc=None,
+        bicg_variant: int = 0) -> dict:
     """Integrate an ``workloads.Ensemble`` on the CPU; returns the final arrays and counters."""
     if systems is not None:
         ens = ens.subset(systems)
@@ -106,6 +108,7 @@ def run(ens, n_periods: int = None, reset_at: int = None, threads: int = 0, syst
         "n_accepted": np.zeros(ns, np.int64), "n_rejected": np.zeros(ns, np.int64),
         "n_bicg_iter": np.zeros(ns, np.int64), "n_rhs": np.zeros(ns, np.int64),
         "status": np.zeros(ns, np.int32),
+        "min_dt": np.full(ns, np.inf),
     }
     P = Problem()
     P.n_systems = ns
@@ -128,6 +131,8 @@ def run(ens, n_periods: int = None, reset_at: int = None, threads: int = 0, syst
     P.algorithm = algorithm
     P.dt0, P.dtmin, P.dtmax, P.grow, P.shrink = ens.dt0, ens.dtmin, ens.dtmax, ens.grow, ens.shrink
     P.bicg_max_iter = bicg_max_iter
+    P.bicg_variant = bicg_variant
+    P.min_dt = _p(a["min_dt"], _dp)
     # the library stages a launch's one shared matrix per CTA (and associates the products
     # accordingly) when the ensemble asks for shared coupling matrices
     P.shared_assoc = int(getattr(ens, "shared_matrices", False) if shared_assoc is None else shared_assoc)

@@ -10,7 +10,7 @@ O = S.ListOfSolverOptions
 
 def run_gpu(ens, n_periods=None, reset_at=None, algorithm=S.Algorithms.RKCK45, ndo=0, do_min_dt=0.0,
             do_save_frequency=1, per_period_solve=False, warps_per_block=0, bicg_max_iter=19, use_graph=True,
-            repeat=1, shared_matrices=False, warps_per_system=0, autotune=False):
+            repeat=1, shared_matrices=False, warps_per_system=0, autotune=False, bicg_recurrence=0):
     n_periods = ens.n_periods if n_periods is None else n_periods
     reset_at = ens.reset_at if reset_at is None else reset_at
     ps = ens.make_solver(algorithm=algorithm, n_dense_output=ndo)
@@ -28,6 +28,8 @@ def run_gpu(ens, n_periods=None, reset_at=None, algorithm=S.Algorithms.RKCK45, n
             ps.SolverOption(O.SharedCouplingMatrices, 1)
         if warps_per_system:
             ps.SolverOption(O.WarpsPerSystem, warps_per_system)
+        if bicg_recurrence:
+            ps.SolverOption(O.BiCGRecurrence, bicg_recurrence)
         for _ in range(repeat - 1):       # earlier solves whose results are discarded (graph capture, replays)
             ps.SynchroniseFromHostToDevice(V.All)
             ps.solve_periods(n_periods, reset_at)

@@ -61,3 +61,75 @@ def test_two_gloo_ranks_reduce_and_shard():
         assert shards[0][2] + shards[1][2] == n
         c0, c1 = shards[0][3], shards[1][3]
         assert abs(c0 - c1) <= 0.05 * (c0 + c1)            # cost-balanced within 5 %
+
+
+def _shard_worker(rank, world, port, out):
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank), MASTER_ADDR="127.0.0.1",
+                      MASTER_PORT=str(port))
+    import datetime
+
+    import torch.distributed as dist
+
+    from bubbleensemble_implicitextension_b200 import sharding as SH
+    from bubbleensemble_implicitextension_b200 import workloads as W
+    from oracle import oracle as O
+
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+    ens = W.c1_ensemble().subset(list(range(0, 256, 21)))
+    ens.max_steps_per_period = 50_000
+    solve = lambda e: O.run(e, n_periods=1, reset_at=-1, threads=1)  # noqa: E731  (the CPU stand-in of a GPU)
+    cost = SH.pilot_costs(ens, rank, world, solve)
+    bounds = SH.cost_bounds(cost, world)
+    part = SH.shard(ens, bounds, rank)
+    res = SH.gather_results(solve(part), rank, world)
+    out[rank] = (bounds.tolist(), cost.tolist(), res)
+    dist.destroy_process_group()
+
+
+@pytest.mark.timeout(600)
+def test_sharded_solve_gathers_the_single_rank_result():
+    """Two gloo ranks: a pilot measures per-system cost, the ensemble is cut into
+    two contiguous cost-balanced shards, each rank integrates its shard (the
+    oracle stands in for the GPU), and the records gathered on rank 0 equal the
+    single-rank run bit for bit."""
+    from bubbleensemble_implicitextension_b200 import sharding as SH
+    from bubbleensemble_implicitextension_b200 import workloads as W
+    from oracle import oracle as O
+
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        out = mgr.dict()
+        port = _free_port()
+        procs = [ctx.Process(target=_shard_worker, args=(r, 2, port, out)) for r in range(2)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(540)
+            assert p.exitcode == 0
+        res = dict(out)
+    bounds, cost, gathered = res[0]
+    assert res[1][2] is None and res[1][0] == bounds
+    ens = W.c1_ensemble().subset(list(range(0, 256, 21)))
+    ens.max_steps_per_period = 50_000
+    whole = O.run(ens, n_periods=1, reset_at=-1)
+    for k in SH.UNIT_KEYS + SH.SYSTEM_KEYS:
+        np.testing.assert_array_equal(gathered[k], np.asarray(whole[k]), err_msg=k)
+    # the cut balances the measured cost to within the cost of one system
+    c = np.asarray(cost)
+    shares = [c[bounds[r]:bounds[r + 1]].sum() for r in range(2)]
+    assert 0 < bounds[1] < ens.n_systems
+    assert max(shares) - min(shares) <= c.max()
+
+
+def test_cost_bounds_properties():
+    from bubbleensemble_implicitextension_b200 import sharding as SH
+    rng = np.random.default_rng(0)
+    for world in (1, 2, 3, 8):
+        for n in (0, 1, 5, 100):
+            c = rng.uniform(0.1, 10.0, n)
+            b = SH.cost_bounds(c, world)
+            assert b[0] == 0 and b[-1] == n and len(b) == world + 1
+            assert (np.diff(b) >= 0).all()
+            if n >= world:
+                shares = [c[b[r]:b[r + 1]].sum() for r in range(world)]
+                assert max(shares) - c.sum() / world <= c.max() + 1e-9

@@ -25,7 +25,7 @@ KEYS = ["state", "uacc", "iuacc", "n_accepted", "n_rejected", "n_bicg_iter", "n_
 class DeviceEnsemble:
     """Every input and output array of an ensemble, in device memory owned by the caller."""
 
-    def __init__(self, ens):
+    def __init__(self, ens, ndo=0):
         import torch
         self.torch = torch
         dev = torch.device("cuda", 0)
@@ -54,6 +54,11 @@ class DeviceEnsemble:
         self.actual_time = torch.empty(ns, dtype=f64, device=dev)
         self.cnt = torch.empty((4, ns), dtype=i64, device=dev)
         self.status = torch.empty(ns, dtype=i32, device=dev)
+        self.ndo = ndo
+        if ndo:
+            self.dense_time = torch.empty((ndo, ns), dtype=f64, device=dev)
+            self.dense_state = torch.empty((ndo, 2, tu), dtype=f64, device=dev)
+            self.dense_index = torch.empty(ns, dtype=i32, device=dev)
         self.errbuf = ctypes.create_string_buffer(512)
 
     def reset(self):
@@ -64,13 +69,18 @@ class DeviceEnsemble:
         self.actual_time.zero_()
         self.cnt.zero_()
         self.status.zero_()
+        if self.ndo:
+            self.dense_time.zero_()
+            self.dense_state.zero_()
+            self.dense_index.zero_()
         torch.cuda.synchronize()
 
-    def problem(self):
+    def problem(self, algorithm=S.Algorithms.RKCK45, do_min_dt=0.0, do_save_frequency=1, options=True,
+                bicg_recurrence=0):
         ens = self.ens
         p = S.NoallocProblem()
         p.n_systems = ens.n_systems
-        p.algorithm = S.Algorithms.RKCK45
+        p.algorithm = algorithm
         p.total_units = ens.total_units
         p.units_host = self.units_host.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
         for name in ("units", "unit_offset", "coupling_offset", "coupling", "state", "upar", "uacc", "iuacc",
@@ -79,9 +89,15 @@ class DeviceEnsemble:
             setattr(p, name, getattr(self, name).data_ptr())
         base, step = self.cnt.data_ptr(), self.cnt.stride(0) * 8
         p.n_accepted, p.n_rejected, p.n_bicg_iter, p.n_rhs = base, base + step, base + 2 * step, base + 3 * step
-        p.dt0, p.dtmin, p.dtmax, p.grow, p.shrink = ens.dt0, ens.dtmin, ens.dtmax, ens.grow, ens.shrink
-        p.bicg_max_iter = 19
+        if self.ndo:
+            for name in ("dense_time", "dense_state", "dense_index"):
+                setattr(p, name, getattr(self, name).data_ptr())
+            p.ndo, p.do_min_dt, p.do_save_frequency = self.ndo, do_min_dt, do_save_frequency
+        if options:   # otherwise left 0: the SolverOption defaults
+            p.dt0, p.dtmin, p.dtmax, p.grow, p.shrink = ens.dt0, ens.dtmin, ens.dtmax, ens.grow, ens.shrink
+            p.bicg_max_iter = 19
         p.max_steps_per_period = ens.max_steps_per_period
+        p.bicg_recurrence = bicg_recurrence
         p.error_message = ctypes.cast(self.errbuf, ctypes.c_char_p)
         p.error_capacity = len(self.errbuf)
         return p
@@ -89,9 +105,13 @@ class DeviceEnsemble:
     def results(self):
         self.torch.cuda.synchronize()
         c = self.cnt.cpu().numpy()
-        return {"state": self.state.cpu().numpy(), "uacc": self.uacc.cpu().numpy(), "iuacc": self.iuacc.cpu().numpy(),
-                "n_accepted": c[0], "n_rejected": c[1], "n_bicg_iter": c[2], "n_rhs": c[3],
-                "status": self.status.cpu().numpy()}
+        out = {"state": self.state.cpu().numpy(), "uacc": self.uacc.cpu().numpy(), "iuacc": self.iuacc.cpu().numpy(),
+               "n_accepted": c[0], "n_rejected": c[1], "n_bicg_iter": c[2], "n_rhs": c[3],
+               "status": self.status.cpu().numpy()}
+        if self.ndo:
+            out.update({"dense_time": self.dense_time.cpu().numpy(), "dense_state": self.dense_state.cpu().numpy(),
+                        "dense_index": self.dense_index.cpu().numpy()})
+        return out
 
 
 def _bounded(ens):
@@ -125,3 +145,63 @@ def test_noalloc_rejects_more_systems_than_its_scratch(gpu):
     p.error_capacity = 256
     assert lib.bes_solve_periods_noalloc(ctypes.byref(p), 1, -1, None) == 1
     assert b"65536" in buf.value
+
+
+def test_noalloc_zero_options_take_the_solver_option_defaults(gpu):
+    """dt0, dtmin, dtmax, grow, shrink and the BiCG cap left 0 mean the reference's
+    SolverOption defaults (Interface.cuh:613-618): the allocating entry point with
+    those defaults set gives the same results."""
+    lib = S.load_library()
+    ens = _bounded(W.c1_ensemble().subset([12, 140]))
+    ens.dt0, ens.dtmin, ens.dtmax, ens.grow, ens.shrink = 1e-2, 1e-12, 1e6, 5.0, 0.1
+    want = run_gpu(ens, n_periods=1, reset_at=-1)
+    dev = DeviceEnsemble(ens)
+    for call in range(2):
+        dev.reset()
+        p = dev.problem(options=False)
+        st = lib.bes_solve_periods_noalloc(ctypes.byref(p), 1, -1, None)
+        assert st == 0, dev.errbuf.value.decode()
+        assert_bitwise(dev.results(), want, KEYS)
+
+
+def test_noalloc_rejects_negative_options(gpu):
+    lib = S.load_library()
+    ens = _bounded(W.c1_ensemble().subset([3]))
+    dev = DeviceEnsemble(ens)
+    dev.reset()
+    p = dev.problem()
+    p.dtmax = -1.0
+    assert lib.bes_solve_periods_noalloc(ctypes.byref(p), 1, -1, None) == 1
+    assert b"dtmax" in dev.errbuf.value
+
+
+def test_noalloc_dense_output_rk4_on_a_caller_stream(gpu):
+    """Dense output and the RK4 stepper, launched on a stream the caller created."""
+    import torch
+    lib = S.load_library()
+    ens = _bounded(W.c1_ensemble().subset([40, 41, 200]))
+    ens.dt0 = 2e-3
+    want = run_gpu(ens, n_periods=2, reset_at=-1, algorithm=S.Algorithms.RK4, ndo=16, do_min_dt=0.05,
+                   do_save_frequency=2)
+    dev = DeviceEnsemble(ens, ndo=16)
+    stream = torch.cuda.Stream()
+    for call in range(2):
+        dev.reset()
+        p = dev.problem(algorithm=S.Algorithms.RK4, do_min_dt=0.05, do_save_frequency=2)
+        st = lib.bes_solve_periods_noalloc(ctypes.byref(p), 2, -1, ctypes.c_void_p(stream.cuda_stream))
+        assert st == 0, dev.errbuf.value.decode()
+        stream.synchronize()
+        assert_bitwise(dev.results(), want, KEYS + ["dense_time", "dense_state", "dense_index"])
+
+
+def test_noalloc_single_reduction_recurrence(gpu):
+    lib = S.load_library()
+    ens = _bounded(ragged_ensemble([32, 64, 20, 128], seed=23))
+    want = run_gpu(ens, n_periods=1, reset_at=-1, bicg_recurrence=1)
+    dev = DeviceEnsemble(ens)
+    for call in range(2):
+        dev.reset()
+        p = dev.problem(bicg_recurrence=1)
+        st = lib.bes_solve_periods_noalloc(ctypes.byref(p), 1, -1, None)
+        assert st == 0, dev.errbuf.value.decode()
+        assert_bitwise(dev.results(), want, KEYS)
