@@ -59,6 +59,11 @@ DATA = "synthetic: seeded PCG64 radii, reference parameter formulas (CollapseStr
 
 WORKLOADS = {
     "c1_period1": WORKLOAD,
+    "c1_full": ("c1_full: configuration 1's horizon -- the 256 systems of c1_period1 (same inputs) integrated for 64 "
+                "acoustic periods from rest, unit accessories reset before period 33 (the first 32 periods discarded, "
+                "CollapseStrength.cu:123-147), collapse records of the last 32; per-period step budget 20000 attempted "
+                "steps (systems that exceed it, the minimum-step cases, are stopped and counted); one step = the 64 "
+                "periods of every system"),
     "c2_period1": ("c2_period1: 16384 systems with N drawn from {4,8,16,32,48,64} (seed 2), one random 3-D cloud per "
                    "system in a 500 um sphere (min separation 20 um), R_E ~ U(1,10) um, dual-frequency drive "
                    "f2 = k f1 (f1 U(20,100) kHz, k in {2,3}, amplitudes U(0,1.5) bar), rtol = atol alternating "
@@ -74,19 +79,30 @@ WORKLOADS = {
                     "RKCK45 rtol=atol=1e-10, FP64 BiCG; one step = one acoustic period of every system from rest"),
     "c5_sweep": ("c5_sweep: the centre 128 x 128 window of the 1024 x 1024 amplitude (0.5-2 bar, linear) x frequency "
                  "(20-200 kHz, log) grid of N = 32 line systems (d = 150 um, R_E ~ U(2,8) um seed 1), 8 periods with the "
-                 "first 4 discarded; plain solver on every point vs the surrogate-screened sweep (solver lattice every "
-                 "4th point, network corrected by the lattice residuals, disagreeing cells integrated, 2% audit); "
-                 "network trained first on 8192 solver runs with random amplitude, frequency and radius draws"),
+                 "first 4 discarded (--sweep-periods, --sweep-discard); plain solver on every point vs the surrogate-"
+                 "screened sweep (solver lattice every 4th point, network corrected by the lattice residuals, "
+                 "disagreeing cells integrated, 2% audit) vs the same screener without the network (bilinear "
+                 "interpolation of the lattice); network trained first on 8192 solver runs with random amplitude, "
+                 "frequency and radius draws"),
+    "c5_strip": ("c5_strip: one row (amplitude 1.25 bar, all 1024 frequencies) and one column (frequency 63.2 kHz, all "
+                 "1024 amplitudes) of the 1024 x 1024 sweep grid of N = 32 line systems, 128 periods with the first 64 "
+                 "discarded; the relative differences of both outputs (collapse strength, max R/R_E) between grid "
+                 "neighbours, the floor for any map served from neighbours"),
 }
 
 
 args_c1_factored = True
 
 
+# periods per bench step and the period before which accessories are reset
+PERIODS = {"c1_full": (64, 32)}
+STEP_BUDGET = {"c1_full": 20_000}
+
+
 def make_ensemble(name, world=1):
     """The workload's ensemble for `world` GPUs (world times the single-GPU size)."""
     from bubbleensemble_implicitextension_b200 import workloads as W
-    if name == "c1_period1":
+    if name in ("c1_period1", "c1_full"):
         return W.c1_ensemble(n_f=16 * world, n_periods=1, reset_at=-1, factored=args_c1_factored)
     if name == "c2_period1":
         return W.c2_ensemble(n_systems=16384 * world, n_periods=1, reset_at=-1)
@@ -113,6 +129,8 @@ def parse():
     ap.add_argument("--sweep-spread", type=float, default=0.05)
     ap.add_argument("--sweep-disagreement", type=float, default=0.02)
     ap.add_argument("--sweep-dump", type=str, default="", help="c5_sweep: write the maps to this .npz")
+    ap.add_argument("--sweep-periods", type=int, default=8, help="c5_sweep: periods per point")
+    ap.add_argument("--sweep-discard", type=int, default=4, help="c5_sweep: periods discarded before recording")
     ap.add_argument("--ref-regcap", choices=["capped", "uncapped"], default="uncapped",
                     help="reference arm: the reference built without its shipped -maxrregcount=128 (the faster of "
                          "the two on the B200: 44.8 vs 30.0 system-periods/s on c1_period1) or with it")
@@ -276,7 +294,8 @@ def run_b200(args, rank, world, local):
     ens_all = make_ensemble(args.workload, world)
     if 0 < args.systems < ens_all.n_systems:
         ens_all = ens_all.subset(list(range(0, ens_all.n_systems, ens_all.n_systems // args.systems))[:args.systems])
-    ens_all.max_steps_per_period = 50_000
+    ens_all.max_steps_per_period = STEP_BUDGET.get(args.workload, 50_000)
+    n_per, reset_at = PERIODS.get(args.workload, (1, -1))
     shard_info = None
     if world > 1:
         # pilot (untimed): one period of an even split per rank gives every system's measured cost
@@ -316,7 +335,7 @@ def run_b200(args, rank, world, local):
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        ps.solve_periods(1, -1)
+        ps.solve_periods(n_per, reset_at)
         e1.record(stream)
         e1.synchronize()
         return e0.elapsed_time(e1), ps.last_solve_launches()
@@ -346,7 +365,7 @@ def run_b200(args, rank, world, local):
     total_ms = sum(times)
     max_ms = allreduce_max(total_ms, world)
     ms_per_step = max_ms / args.steps
-    value = ens_all.n_systems * args.steps / (max_ms * 1e-3)
+    value = ens_all.n_systems * n_per * args.steps / (max_ms * 1e-3)
 
     # end to end through the public API: host inputs -> H2D -> solve -> D2H of the results
     in_bytes = ens.state.nbytes + init_uacc.nbytes + init_iuacc.nbytes
@@ -363,7 +382,7 @@ def run_b200(args, rank, world, local):
         ps.SynchroniseFromHostToDevice(V.ActualState)
         ps.SynchroniseFromHostToDevice(V.UnitAccessories)
         ps.SynchroniseFromHostToDevice(V.IntegerUnitAccessories)
-        ps.solve_periods(1, -1)
+        ps.solve_periods(n_per, reset_at)
         ps.SynchroniseFromDeviceToHost(V.ActualState)
         ps.SynchroniseFromDeviceToHost(V.UnitAccessories)
         ps.SynchroniseFromDeviceToHost(V.IntegerUnitAccessories)
@@ -374,7 +393,7 @@ def run_b200(args, rank, world, local):
         if it >= args.warmup:
             e2e_times.append(time.perf_counter() - t0)
     e2e_max = allreduce_max(sum(e2e_times), world)
-    e2e_value = ens_all.n_systems * args.steps / e2e_max
+    e2e_value = ens_all.n_systems * n_per * args.steps / e2e_max
     # the shards' result records on rank 0 (after the timed regions)
     c_last = ps.counters()
     local_rec = {"state": ps.get_array(V.ActualState).reshape(2, -1), "uacc": ps.get_array(V.UnitAccessories).reshape(64, -1),
@@ -395,7 +414,7 @@ def run_b200(args, rank, world, local):
         "config": {"workload": WORKLOADS[args.workload], "systems": ens_all.n_systems,
                    "units_per_system": int(ens.units[0]) if len(set(ens.units.tolist())) == 1 else "mixed",
                    "total_units": ens.total_units,
-                   "periods_per_step": 1,
+                   "periods_per_step": n_per,
                    "coupling_input": ("shared symmetric geometry G = 1/d with unit factors R^-2, R^3"
                                       if ens.coupling_row_scale is not None else "per-ensemble matrix as given"),
                    "warps_per_system": "one" if args.warps_per_system else "2 or 4 above 32 units",
@@ -418,8 +437,12 @@ def run_b200(args, rank, world, local):
         "clocks": clk,
         "counters": {"attempted_steps": int(attempted.sum()), "max_attempted_steps": int(attempted.max()),
                      "bicg_iterations": int(c["bicg"].sum()), "status_or": int(np.bitwise_or.reduce(c["status"])),
-                     "systems_at_step_budget": int(((c["status"] & 4) > 0).sum()),
-                     "step_budget_per_period": int(ens.max_steps_per_period)},
+                     "systems_at_step_budget": int(((gathered["status"] & 4) > 0).sum()),
+                     "step_budget_per_period": int(ens.max_steps_per_period),
+                     # systems stopped by the step budget have no valid result: throughput over the others
+                     "completed_systems": int(((gathered["status"] & 4) == 0).sum()),
+                     "completed_system_periods_per_s": float(((gathered["status"] & 4) == 0).sum() * n_per * args.steps
+                                                             / (max_ms * 1e-3))},
     }
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(ens, args.cpu_sample_systems)
@@ -450,18 +473,21 @@ def run_reference(args, rank, world):
     if args.workload == "c2_period1":
         return {"impl": "reference", "unavailable": "the reference solver takes one unit count (template UPS) and one "
                 "global coupling matrix; c2_period1 has per-system sizes and geometries"}
-    if args.workload == "c3_period1":
-        return {"impl": "reference", "unavailable": "no reference harness built for 4096 systems x 128 units"}
     if args.workload == "c3r_period1":
         return {"impl": "reference", "unavailable": "the reference takes one global coupling matrix; per-system "
                 "radii over a shared geometry have no reference form (oracle-only)"}
     from bubbleensemble_implicitextension_b200 import workloads as W
     from oracle import build_ref, ref_io
 
-    exe = build_ref.path(32, 256, 0, args.ref_regcap == "capped")
+    capped = args.ref_regcap == "capped"
+    if args.workload == "c3_period1":
+        # configuration 3 variant (i) as the reference stores it: one global matrix C_ij = R_j^3 / (R_i^2 d_ij)
+        ens, ups, ns_max, name = W.c3_ensemble(n_periods=1, reset_at=-1, factored=False), 128, 4096, "c3_period1"
+    else:
+        ens, ups, ns_max, name = W.c1_ensemble(n_periods=1, reset_at=-1), 32, 256, "c1_period1"
+    exe = build_ref.path(ups, ns_max, 0, capped)
     if not exe.exists():
         return {"impl": "reference", "unavailable": f"{exe.name} was not built (the reference tree was absent at build time)"}
-    ens = W.c1_ensemble(n_periods=1, reset_at=-1)
     n = args.warmup + args.steps
     clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
     clocks.start()
@@ -474,13 +500,15 @@ def run_reference(args, rank, world):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * per.mean(), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": DATA, "impl": "reference",
-        "config": {"workload": WORKLOAD, "systems": ens.n_systems, "units_per_system": 32, "periods_per_step": 1,
+        "config": {"workload": WORKLOADS[name], "systems": ens.n_systems, "units_per_system": ups,
+                   "periods_per_step": 1,
+                   "coupling_input": "the reference-format matrix C_ij = R_j^3 / (R_i^2 d_ij), one global matrix",
                    "l2": "inputs re-set through SetHost + SynchroniseFromHostToDevice before every period (untimed)",
                    "parallelism": "reference ProblemSolver, one GPU"},
         "cpu_baseline": {"value": value, "unit": UNIT, "kind": "reference", "cores": 1,
-                         "sample": "the reference's own per-block CUDA solver (ProblemSolver<256,32,...,RKCK45,double>, "
-                                   "unmodified headers, nvcc -O3 sm_100a, " + ("-maxrregcount=128 as shipped"
-                                   if args.ref_regcap == "capped" else "without the shipped register cap") + ") on the same GPU, "
+                         "sample": f"the reference's own per-block CUDA solver (ProblemSolver<{ns_max},{ups},...,RKCK45,"
+                                   "double>, unmodified headers, nvcc -O3 sm_100a, " + ("-maxrregcount=128 as shipped"
+                                   if capped else "without the shipped register cap") + ") on the same GPU, "
                                    "timed per Solve() with the host thread waiting on its event; the reference "
                                    "has no CPU implementation"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -498,7 +526,7 @@ def run_sweep(args, rank, world, local):
     if rank != 0:
         return None
     torch.cuda.set_device(local)
-    n_grid, win, n_per, reset = 1024, args.sweep_window, 8, 4
+    n_grid, win, n_per, reset = 1024, args.sweep_window, args.sweep_periods, args.sweep_discard
     pa_full = W.linspace_ref(0.5, 2.0, n_grid)
     f_full = np.logspace(np.log10(20.0), np.log10(200.0), n_grid)
     lo = (n_grid - win) // 2
@@ -527,6 +555,11 @@ def run_sweep(args, rank, world, local):
     res = SG.screen_sweep_lattice(net, pa, fr, radii, solve, stride=args.sweep_stride,
                                   cell_spread=args.sweep_spread, cell_disagreement=args.sweep_disagreement)
     net.close()
+    # the same screener without the network (what the network adds is the difference)
+    res0 = SG.screen_sweep_lattice(None, pa, fr, radii, solve, stride=args.sweep_stride,
+                                   cell_spread=args.sweep_spread, cell_disagreement=args.sweep_disagreement)
+    served0 = ~res0.integrated
+    e0_s = np.abs(10.0 ** res0.map[..., 0] - 10.0 ** plain[..., 0]) / 10.0 ** plain[..., 0]
     served = ~res.integrated
     s_true = 10.0 ** plain[..., 0]
     e_s = np.abs(10.0 ** res.map[..., 0] - s_true) / s_true
@@ -554,15 +587,72 @@ def run_sweep(args, rank, world, local):
                   "meets_1pct_max_error": bool(q(e_s, 1.0) <= 0.01),
                   "audit_max_rel_error": res.audit_max_rel_error,
                   "integrated_points_equal_plain": same,
-                  "network_training_s": train_s, "training_data_solver_s": gen_s},
+                  "network_training_s": train_s, "training_data_solver_s": gen_s,
+                  "without_network": {"screened_s": res0.seconds, "speedup": plain_s / res0.seconds,
+                                      "integrated_fraction": float(res0.integrated.mean()),
+                                      "served_strength_rel_error": {
+                                          "max": float(e0_s[served0].max()) if served0.any() else 0.0,
+                                          "p99": float(np.quantile(e0_s[served0], 0.99)) if served0.any() else 0.0,
+                                          "mean": float(e0_s[served0].mean()) if served0.any() else 0.0}},
+                  "periods": n_per, "discarded": reset,
+                  "verification": "integrated points (lattice, flagged cells, audit) are the solver's values; "
+                                  "served points are not integrated (screen_sweep_lattice(verify=True) integrates "
+                                  "them too, which costs the plain sweep's time)"},
         "gpu_launches": None,
     }
+
+
+def run_strip(args, rank, world, local):
+    """Neighbour differences of both sweep outputs along one row and one column of the 1024 x 1024 grid."""
+    import torch
+
+    from bubbleensemble_implicitextension_b200 import surrogate as SG
+    from bubbleensemble_implicitextension_b200 import workloads as W
+
+    if rank != 0:
+        return None
+    torch.cuda.set_device(local)
+    n_grid, n_per, reset = 1024, 128, 64
+    pa_full = W.linspace_ref(0.5, 2.0, n_grid)
+    f_full = np.logspace(np.log10(20.0), np.log10(200.0), n_grid)
+    radii = np.random.default_rng(1).uniform(2.0, 8.0, 32)
+    mid = n_grid // 2
+    pts_pa = np.r_[np.full(n_grid, pa_full[mid]), pa_full]
+    pts_f = np.r_[f_full, np.full(n_grid, f_full[mid])]
+    ens = SG.line_ensemble(pts_pa, pts_f, np.broadcast_to(radii, (len(pts_pa), 32)), n_periods=n_per, reset_at=reset)
+    t0 = time.perf_counter()
+    Y, status, _ = SG.solve_ensemble(ens, max_steps=20_000)
+    seconds = time.perf_counter() - t0
+    ok = (status & 4) == 0
+    out = {}
+    for name, sl in (("frequency_direction", slice(0, n_grid)), ("amplitude_direction", slice(n_grid, 2 * n_grid))):
+        y, g = Y[sl], ok[sl]
+        both = g[1:] & g[:-1]
+        s = 10.0 ** y[:, 0]
+        ds = np.abs(s[1:] - s[:-1]) / np.minimum(s[1:], s[:-1])
+        dr = np.abs(y[1:, 1] - y[:-1, 1]) / np.minimum(np.abs(y[1:, 1]), np.abs(y[:-1, 1])).clip(1e-12)
+
+        def q(v):
+            return {"median": float(np.median(v[both])), "p90": float(np.quantile(v[both], 0.9)),
+                    "max": float(v[both].max())}
+        out[name] = {"collapse_strength": q(ds), "max_radius": q(dr), "neighbour_pairs": int(both.sum())}
+    return {"metric": "relative difference between sweep-grid neighbours",
+            "value": out["frequency_direction"]["collapse_strength"]["median"], "unit": "relative",
+            "higher_is_better": False, "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": 1e3 * seconds,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
+            "config": {"workload": WORKLOADS["c5_strip"], "points": int(len(pts_pa)),
+                       "systems_at_step_budget": int((~ok).sum())},
+            "strip": out, "gpu_launches": None}
 
 
 def main():
     args = parse()
     rank, world, local = dist_init(args.gpus)
-    if args.workload == "c5_sweep":
+    if args.workload == "c5_strip":
+        line = run_strip(args, rank, world, local) if args.impl == "b200" else (
+            {"impl": "reference", "unavailable": "a measurement of the map's roughness, not a solver workload"}
+            if rank == 0 else None)
+    elif args.workload == "c5_sweep":
         line = (run_sweep(args, rank, world, local) if args.impl == "b200" else
                 ({"impl": "reference", "unavailable": "the reference has no surrogate; the plain solver arm of the "
                   "sweep is timed in the same line"} if rank == 0 else None))

@@ -470,20 +470,21 @@ __device__ __forceinline__ int bicg_iterate(const Sys<U, G>& S, const DeviceProb
 #pragma unroll
         for (int m = 0; m < U; m++) prod[m] = r[m] * rt[m];
         double rho1 = grp_tree_sum<U, G>(S, prod);
-        double rho2 = 0.0;
+        double rho2 = 0.0, y2 = 0.0;   /* y2: reciprocal estimate of rho2, formed an iteration early */
         for (int iter = 1; iter <= P.bicg_max_iter; iter++) {
             if (iter == 1) {
 #pragma unroll
                 for (int m = 0; m < U; m++) { p[m] = r[m]; pt[m] = rt[m]; }
                 if (fabs(rho1) < 1e-6) { exited = true; break; }
             } else {
-                const double beta = rho1 / rho2;
+                const double beta = math::div_known(rho1, rho2, y2);   /* = rho1 / rho2 */
 #pragma unroll
                 for (int m = 0; m < U; m++) {
                     p[m] = fma(beta, p[m], r[m]);
                     pt[m] = fma(beta, pt[m], rt[m]);
                 }
             }
+            const double y1 = math::recip_estimate(rho1);   /* becomes y2 at the end of the iteration */
             apply(p, pt, q, qt);
 #pragma unroll
             for (int m = 0; m < U; m++) prod[m] = pt[m] * q[m];
@@ -499,13 +500,14 @@ __device__ __forceinline__ int bicg_iterate(const Sys<U, G>& S, const DeviceProb
             double rho_next;
             const bool small = grp_sum_max_below<U, G>(S, ar, prod, 1e-6, rho_next);
             rho2 = rho1;
+            y2 = y1;
             done++;
             if (small) { exited = true; break; }
             rho1 = rho_next;
         }
     } else {
         double w[U], wt[U], rw[U];
-        double sigma = 0.0, rho_prev = 0.0;
+        double sigma = 0.0, rho_prev = 0.0, y_prev = 0.0;   /* y_prev: reciprocal estimate of rho_prev */
         for (int iter = 1; iter <= P.bicg_max_iter; iter++) {
             apply(r, rt, w, wt);
 #pragma unroll
@@ -523,7 +525,7 @@ __device__ __forceinline__ int bicg_iterate(const Sys<U, G>& S, const DeviceProb
                 for (int m = 0; m < U; m++) { p[m] = r[m]; pt[m] = rt[m]; q[m] = w[m]; qt[m] = wt[m]; }
                 sigma = mu;
             } else {
-                const double beta = rho / rho_prev;
+                const double beta = math::div_known(rho, rho_prev, y_prev);   /* = rho / rho_prev */
                 sigma = fma(-(beta * beta), sigma, mu);
 #pragma unroll
                 for (int m = 0; m < U; m++) {
@@ -535,6 +537,7 @@ __device__ __forceinline__ int bicg_iterate(const Sys<U, G>& S, const DeviceProb
             }
             const double alpha = rho / sigma;
             rho_prev = rho;
+            y_prev = math::recip_estimate(rho);
 #pragma unroll
             for (int m = 0; m < U; m++) {
                 x[m] = fma(alpha, p[m], x[m]);

@@ -279,8 +279,11 @@ class LatticeScreenResult:
     lattice: np.ndarray        # bool [n_pa, n_f]: lattice points
     audited: np.ndarray        # bool [n_pa, n_f]: audit points outside flagged cells
     audit_max_rel_error: float # corrected-network error on the audit points, collapse strength
-    solve_seconds: float       # time inside the solver (both passes)
-    seconds: float             # whole screened sweep
+    solve_seconds: float       # time inside the solver (all passes)
+    seconds: float             # whole screened sweep (without the verification pass)
+    served_map: Optional[np.ndarray] = None     # with verify: what the screener would have served [n_pa, n_f, 2]
+    verify_seconds: float = 0.0                 # with verify: the pass that integrates every served point
+    served_rel_error: Optional[np.ndarray] = None  # with verify: |served - solver| / solver per point, strength
 
 
 def _lattice_axis(n: int, stride: int):
@@ -292,10 +295,10 @@ def _lattice_axis(n: int, stride: int):
     return idx, cell, t
 
 
-def screen_sweep_lattice(mlp: "MLP", pa: np.ndarray, f_khz: np.ndarray, radii_um: np.ndarray,
+def screen_sweep_lattice(mlp: Optional["MLP"], pa: np.ndarray, f_khz: np.ndarray, radii_um: np.ndarray,
                          solve: Callable[[np.ndarray, np.ndarray], np.ndarray], stride: int = 4,
                          cell_spread: float = 0.05, cell_disagreement: float = 0.02,
-                         audit_fraction: float = 0.02, seed: int = 0) -> LatticeScreenResult:
+                         audit_fraction: float = 0.02, seed: int = 0, verify: bool = False) -> LatticeScreenResult:
     """Multi-fidelity sweep: solver lattice + network corrected by the lattice residuals.
 
     `solve(pa_points, f_points)` returns the solver's outputs [n, 2] (log10
@@ -304,7 +307,15 @@ def screen_sweep_lattice(mlp: "MLP", pa: np.ndarray, f_khz: np.ndarray, radii_um
     the corrected network strength differs from the bilinear interpolation of
     the corner solutions by more than `cell_disagreement` (relative) anywhere
     inside it; a random `audit_fraction` of the other points is integrated too
-    and measures the error of what is served."""
+    and measures the error of what is served.
+
+    mlp=None is the same screener without the network: the served values are
+    the bilinear interpolation of the lattice solutions and only the corner
+    spread flags cells (what the network adds is the difference between the
+    two runs).  verify=True integrates every served point as well, after the
+    screened map is complete: the map returned is then the solver's everywhere,
+    served_map and served_rel_error record what the screener had served and
+    how far it was off, and verify_seconds the cost of that pass."""
     t0 = time.perf_counter()
     n_pa, n_f = len(pa), len(f_khz)
     PA, FR = np.meshgrid(pa, f_khz, indexing="ij")
@@ -317,7 +328,10 @@ def screen_sweep_lattice(mlp: "MLP", pa: np.ndarray, f_khz: np.ndarray, radii_um
     sol = np.zeros((n_pa, n_f, 2))
     sol[lat] = solve(PA[lat], FR[lat])
     solve_s += time.perf_counter() - t1
-    pred = mlp.predict(features(PA.ravel(), FR.ravel(), radii_um)).reshape(n_pa, n_f, 2).astype(np.float64)
+    if mlp is not None:
+        pred = mlp.predict(features(PA.ravel(), FR.ravel(), radii_um)).reshape(n_pa, n_f, 2).astype(np.float64)
+    else:
+        pred = np.zeros((n_pa, n_f, 2))   # no network: the residuals are the lattice solutions themselves
     res = np.where(lat[..., None], sol - pred, 0.0)
     # bilinear interpolation inside each cell: corners (a, b), (a+1, b), (a, b+1), (a+1, b+1)
     A0, A1 = ia[ca][:, None], ia[ca + 1][:, None]
@@ -356,5 +370,18 @@ def screen_sweep_lattice(mlp: "MLP", pa: np.ndarray, f_khz: np.ndarray, radii_um
     if audit.any():
         s_true = 10.0 ** sol[audit][:, 0]
         err = float(np.max(np.abs(10.0 ** corr[audit][:, 0] - s_true) / s_true))
-    return LatticeScreenResult(map=out, integrated=integrated, lattice=lat, audited=audit,
-                               audit_max_rel_error=err, solve_seconds=solve_s, seconds=time.perf_counter() - t0)
+    seconds = time.perf_counter() - t0
+    result = LatticeScreenResult(map=out, integrated=integrated, lattice=lat, audited=audit,
+                                 audit_max_rel_error=err, solve_seconds=solve_s, seconds=seconds)
+    if verify:
+        served = ~integrated
+        t1 = time.perf_counter()
+        checked = sol.copy()
+        if served.any():
+            checked[served] = solve(PA[served], FR[served])
+        result.verify_seconds = time.perf_counter() - t1
+        s_true = 10.0 ** checked[..., 0]
+        result.served_rel_error = np.where(served, np.abs(10.0 ** out[..., 0] - s_true) / s_true, 0.0)
+        result.served_map = out
+        result.map = checked
+    return result

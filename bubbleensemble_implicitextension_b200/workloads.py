@@ -141,6 +141,7 @@ class Ensemble:
     shared_matrices: bool = False     # SharedCouplingMatrices: stage the launch's one matrix per CTA
     coupling_row_scale: Optional[np.ndarray] = None   # [TU] a_i of C_ij = a_i G_ij b_j (shared geometry G)
     coupling_col_scale: Optional[np.ndarray] = None   # [TU] b_j
+    band_width: int = 0               # CBW: > 0, only the wrapping band of 2 CBW + 1 diagonals couples
     name: str = ""
     info: dict = dataclasses.field(default_factory=dict)
 
@@ -197,6 +198,8 @@ class Ensemble:
 
     def make_solver(self, device: int = 0, **kw) -> S.ProblemSolver:
         """Create a ProblemSolver filled with this ensemble (host mirrors only; call H2D)."""
+        if self.band_width and "coupling_bandwidth" not in kw:
+            kw["coupling_bandwidth"] = self.band_width
         ps = S.ProblemSolver(self.n_systems, self.units if len(set(self.units.tolist())) > 1 else int(self.units[0]),
                              n_coupling_matrices=self.n_matrices, coupling_matrix_of_system=self.matrix_of_system,
                              device=device, **kw)
@@ -396,6 +399,39 @@ def c3_radii_ensemble(n_systems: int = 4096, n_units: int = 128, seed: int = 3, 
                     rtol=np.full((2, n_systems), rtol), atol=np.full((2, n_systems), rtol), n_periods=n_periods,
                     reset_at=reset_at, shared_matrices=True, coupling_row_scale=1.0 / (r * r),
                     coupling_col_scale=r * r * r, name=f"c3_radii_{n_systems}x{n_units}")
+
+
+def ring_ensemble(n_systems: int = 64, n_units: int = 128, band_width: int = 1, seed: int = 4,
+                  spacing_um: float = 120.0, pa_range=(0.8, 1.4), f_khz: float = 80.0, rtol: float = 1e-10,
+                  n_periods: int = 1, reset_at: int = -1) -> Ensemble:
+    """Bubbles on a ring, each coupled to its `band_width` neighbours on either
+    side only: C_ij = R_j^3 / (R_i^2 d_ij) for (j - i) mod N within the band,
+    d the chord distance on a circle whose neighbour spacing is `spacing_um`,
+    zero elsewhere -- the reference's banded storage (CBW = band_width, a
+    wrapping band of 2 CBW + 1 diagonals).  One radius draw (U(2, 8) um,
+    PCG64(seed)) per system, amplitudes spread over pa_range."""
+    rng = np.random.default_rng(seed)
+    n = n_units
+    ang = 2.0 * np.pi * np.arange(n) / n
+    rad = spacing_um / (2.0 * np.sin(np.pi / n))
+    pos = np.stack([rad * np.cos(ang), rad * np.sin(ang)], 1)
+    d = np.sqrt(((pos[:, None, :] - pos[None, :, :]) ** 2).sum(-1))
+    off = (np.arange(n)[None, :] - np.arange(n)[:, None]) % n
+    in_band = ((off <= band_width) | (off >= n - band_width)) & (off != 0)
+    blocks, ups = [], []
+    pa = np.linspace(pa_range[0], pa_range[1], n_systems)
+    for s in range(n_systems):
+        r = rng.uniform(2.0, 8.0, n)
+        C = np.where(in_band, r[None, :] ** 3 / (r[:, None] ** 2 * np.where(in_band, d, 1.0)), 0.0)
+        blocks.append(C.T.reshape(-1))
+        ups.append(km_unit_parameters(pa[s], f_khz, 0.0, 0.0, 0.0, r))
+    state = np.zeros((2, n_systems * n))
+    state[0] = 1.0
+    return Ensemble(units=np.full(n_systems, n, dtype=np.int32), upar=np.concatenate(ups, 1), state=state,
+                    coupling=np.concatenate(blocks), matrix_of_system=np.arange(n_systems, dtype=np.int32),
+                    rtol=np.full((2, n_systems), rtol), atol=np.full((2, n_systems), rtol), n_periods=n_periods,
+                    reset_at=reset_at, band_width=band_width, name=f"ring_{n_systems}x{n}_bw{band_width}",
+                    info={"pa_bar": pa, "f_khz": np.full(n_systems, f_khz)})
 
 
 def explicit_matrices(ens: Ensemble) -> Ensemble:

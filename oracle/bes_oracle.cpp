@@ -136,8 +136,21 @@ struct Work {
 int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
                 const double* up, long ups, const double* C, int max_iter,
                 double* f0, double* f1, bool* capped, bool shared_assoc = false,
-                const double* ra = nullptr, const double* cb = nullptr, bool symmetric = false, int variant = 0) {
+                const double* ra = nullptr, const double* cb = nullptr, bool symmetric = false, int variant = 0,
+                int bw = 0) {
     const int N = w.N;
+    /* banded association (bw > 0, 2 bw + 1 < N): only the wrapping band
+     * j = i + d - bw (mod N), d = 0 .. 2 bw, of C is read, with four chains over
+     * d (d mod 4); W is kept by diagonal, Wb[d][i] = W[i][j(i, d)], and the
+     * transposed product of unit i sums Wb[d][k] vt[k] over k = i + bw - d (mod N) */
+    const bool band = bw > 0 && 2 * bw + 1 < N && !shared_assoc;
+    const int nd = 2 * bw + 1;
+    auto jband = [&](int i, int d) { int j = i + d - bw; if (j < 0) j += N; if (j >= N) j -= N; return j; };
+    auto band_sum4 = [&](auto term) {
+        double c[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int d = 0; d < nd; d++) term(d, c[d & 3]);
+        return (c[0] + c[1]) + (c[2] + c[3]);
+    };
     double upl[NUP];
     for (int i = 0; i < N; i++) {
         for (int k = 0; k < NUP; k++) upl[k] = up[(long)k * ups + i];
@@ -155,6 +168,23 @@ int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
     /* b = rD (C CPT) + x_u ; r = b - A x_u  (Steppers.cuh:495-505, :576-584, :647-666) */
     for (int i = 0; i < N; i++) {
         double bi, ax;
+        if (band) {
+            bi = band_sum4([&](int d, double& acc) { const int j = jband(i, d); acc = fma(C[i + (long)j * N], w.cpt[j], acc); });
+            bi = fma(w.rd[i], bi, w.xu[i]);
+            ax = band_sum4([&](int d, double& acc) {
+                const int j = jband(i, d);
+                acc = fma(C[i + (long)j * N] * w.x1sq[j], w.xu[j], acc);
+            });
+            ax = fma(w.rd[i], ax, w.xu[i]);
+            w.r[i] = bi - ax;
+            w.rt[i] = w.r[i];
+            w.x[i] = w.xu[i];
+            for (int d = 0; d < nd; d++) {
+                const int j = jband(i, d);
+                w.W[i + (long)d * N] = (w.rd[i] * C[i + (long)j * N]) * w.x1sq[j];   /* Wb[d][i] */
+            }
+            continue;
+        }
         if (shared_assoc) {
             bi = row_sum4(N, [&](int j) { return C[i + (long)j * N]; }, [&](int j) { return w.tmp2[j]; });
             bi = fma(w.vs[i], bi, w.xu[i]);
@@ -174,6 +204,16 @@ int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
     /* q = A v (row sums) and qt = A^T vt (tree sums or, for a symmetric shared
      * matrix, row sums), Steppers.cuh:669-706 */
     auto apply = [&](const double* v, const double* vt, double* q, double* qt) {
+        if (band) {
+            for (int i = 0; i < N; i++) {
+                q[i] = v[i] + band_sum4([&](int d, double& acc) { acc = fma(w.W[i + (long)d * N], v[jband(i, d)], acc); });
+                qt[i] = vt[i] + band_sum4([&](int d, double& acc) {
+                    const int k = jband(i, 2 * bw - d);   /* k = i + bw - d */
+                    acc = fma(w.W[k + (long)d * N], vt[k], acc);
+                });
+            }
+            return;
+        }
         if (shared_assoc) {
             for (int j = 0; j < N; j++) { w.z[j] = w.us[j] * v[j]; w.zt[j] = w.vs[j] * vt[j]; }
         }
@@ -330,7 +370,7 @@ struct SystemRun {
                              P->shared_assoc != 0 && (N > 32 || symmetric_C),
                              P->coupling_row_scale ? P->coupling_row_scale + off : nullptr,
                              P->coupling_col_scale ? P->coupling_col_scale + off : nullptr, symmetric_C,
-                             P->bicg_variant);
+                             P->bicg_variant, P->band_width);
         nbicg += it;
         if (capped) capped_any = true;
         return it;

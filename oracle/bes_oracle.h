@@ -90,6 +90,11 @@ typedef struct bes_oracle_problem {
     /* optional [n_systems] output, or NULL: the smallest step size attempted
      * (min over the periods of this call and the value already stored) */
     double* min_dt;
+    /* > 0: the coupling matrices are banded (2 band_width + 1 wrapping
+     * diagonals, the reference's CBW storage) and systems with
+     * 2 band_width + 1 < N use the banded association (see coupled_rhs) */
+    int32_t band_width;
+    int32_t pad2;
 } bes_oracle_problem;
 
 /* Integrate `n_periods` reference Solve() calls for every active system.

@@ -37,6 +37,7 @@ VARIANTS = [
     (32, 64, 16, True),
     (64, 64, 0, True),
     (128, 16, 0, True),
+    (128, 4096, 0, True), (128, 4096, 0, False),   # configuration 3: 4096 systems sharing one matrix
 ]
 
 

@@ -37,6 +37,7 @@ class Problem(ctypes.Structure):
         ("n_accepted", _i64p), ("n_rejected", _i64p), ("n_bicg_iter", _i64p), ("n_rhs", _i64p),
         ("status", _i32p), ("coupling_row_scale", _dp), ("coupling_col_scale", _dp),
         ("bicg_variant", ctypes.c_int32), ("pad", ctypes.c_int32), ("min_dt", _dp),
+        ("band_width", ctypes.c_int32), ("pad2", ctypes.c_int32),
     ]
 
 
@@ -82,7 +83,7 @@ def _p(a, t):
 def run(ens, n_periods: int = None, reset_at: int = None, threads: int = 0, systems=None,
         algorithm: int = 1, ndo: int = 0, do_min_dt: float = 0.0, do_save_frequency: int = 1,
         bicg_max_iter: int = 19, uacc=None, iuacc=None, state=None, shared_assoc=None,
-        bicg_variant: int = 0) -> dict:
+        bicg_variant: int = 0, band_width=None) -> dict:
     """Integrate an ``workloads.Ensemble`` on the CPU; returns the final arrays and counters."""
     if systems is not None:
         ens = ens.subset(systems)
@@ -132,6 +133,8 @@ def run(ens, n_periods: int = None, reset_at: int = None, threads: int = 0, syst
     P.dt0, P.dtmin, P.dtmax, P.grow, P.shrink = ens.dt0, ens.dtmin, ens.dtmax, ens.grow, ens.shrink
     P.bicg_max_iter = bicg_max_iter
     P.bicg_variant = bicg_variant
+    # banded coupling storage (the reference's CBW): the banded association where 2 bw + 1 < N
+    P.band_width = int(getattr(ens, "band_width", 0) if band_width is None else band_width)
     P.min_dt = _p(a["min_dt"], _dp)
     # the library stages a launch's one shared matrix per CTA (and associates the products
     # accordingly) when the ensemble asks for shared coupling matrices

@@ -66,3 +66,37 @@ def test_audit_points_are_integrated_and_measured():
     assert res.integrated[res.audited].all()
     assert np.array_equal(res.map[res.audited], truth[res.audited])
     assert 0.0 <= res.audit_max_rel_error < 0.01
+
+
+def test_without_network_serves_the_lattice_interpolation():
+    """mlp=None: the counterfactual screener (bilinear interpolation of the lattice,
+    corner-spread criterion only) -- the baseline the network is measured against."""
+    pa, f = _grid()
+    PA, FR = np.meshgrid(pa, f, indexing="ij")
+    truth = _map(PA.ravel(), FR.ravel(), False).reshape(len(pa), len(f), 2)
+    res = SG.screen_sweep_lattice(None, pa, f, np.full(32, 5.0), lambda pp, ff: _map(pp, ff, False), stride=4,
+                                  cell_spread=0.5, cell_disagreement=0.05, audit_fraction=0.0)
+    assert np.array_equal(res.map[res.integrated], truth[res.integrated])
+    # the analytic map is linear in pa and in log10 f but not in f itself: interpolation errs a little
+    served = ~res.integrated
+    err = np.abs(10 ** res.map[served][:, 0] - 10 ** truth[served][:, 0]) / 10 ** truth[served][:, 0]
+    assert 0.0 < err.max() < 0.05
+
+
+def test_verify_integrates_every_served_point():
+    pa, f = _grid()
+    calls = []
+
+    def solve(pp, ff):
+        calls.append(len(pp))
+        return _map(pp, ff, True)
+
+    res = SG.screen_sweep_lattice(_Net(), pa, f, np.full(32, 5.0), solve, stride=4, cell_spread=0.5,
+                                  cell_disagreement=0.05, audit_fraction=0.0, verify=True)
+    PA, FR = np.meshgrid(pa, f, indexing="ij")
+    truth = _map(PA.ravel(), FR.ravel(), True).reshape(len(pa), len(f), 2)
+    assert np.array_equal(res.map, truth)                       # the verified map is the solver's everywhere
+    assert sum(calls) == len(pa) * len(f)                       # every point integrated exactly once
+    served = ~res.integrated
+    assert np.allclose(res.served_map[res.integrated], truth[res.integrated])
+    assert (res.served_rel_error[res.integrated] == 0).all() and res.served_rel_error[served].max() < 0.02

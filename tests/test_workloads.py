@@ -29,3 +29,27 @@ def test_shard_bounds_cover_every_system_once(world):
     b = W.shard_bounds(units, world)
     assert len(b) == world + 1 and b[0] == 0 and b[-1] == len(units)
     assert np.all(np.diff(b) >= 0)
+
+
+def test_ring_ensemble_is_banded():
+    from bubbleensemble_implicitextension_b200 import workloads as W
+    ens = W.ring_ensemble(n_systems=3, n_units=40, band_width=2)
+    n = 40
+    for s in range(3):
+        C = ens.coupling[s * n * n:(s + 1) * n * n].reshape(n, n).T
+        off = (np.arange(n)[None, :] - np.arange(n)[:, None]) % n
+        band = ((off <= 2) | (off >= n - 2)) & (off != 0)
+        assert (C[band] > 0).all() and (C[~band] == 0).all()
+    assert ens.band_width == 2
+
+
+def test_oracle_banded_association_matches_full_matrix(oracle_lib):
+    """The banded association (band products over the 2 CBW + 1 diagonals only)
+    and the full-matrix association of the same banded matrix agree to rounding."""
+    from bubbleensemble_implicitextension_b200 import workloads as W
+    ens = W.ring_ensemble(n_systems=2, n_units=64, band_width=2)
+    ens.max_steps_per_period = 50_000
+    a = oracle_lib.run(ens, band_width=2)
+    b = oracle_lib.run(ens, band_width=0)
+    np.testing.assert_array_equal(a["iuacc"], b["iuacc"])
+    assert (np.abs(a["state"][0] - b["state"][0]) / b["state"][0]).max() < 1e-10
