@@ -77,6 +77,10 @@ WORKLOADS = {
                     "once per CTA), each system with its own radii (lognormal median 4 um sigma 0.4 clipped to "
                     "[1,12] um, seed 3+s) through the unit factors a_i = R_i^-2, b_j = R_j^3, 200 kHz at 1.2 bar, "
                     "RKCK45 rtol=atol=1e-10, FP64 BiCG; one step = one acoustic period of every system from rest"),
+    "ring_period1": ("ring_period1: 1024 systems, each a ring of 128 Keller-Miksis bubbles (120 um neighbour spacing, "
+                     "R_E ~ U(2,8) um per system, 80 kHz, 0.8-1.4 bar) coupled to its nearest neighbour on either side "
+                     "only -- the reference's banded storage with CBW = 1 -- RKCK45 rtol=atol=1e-10; the banded "
+                     "operator (3 diagonals) unless --ring-full; one step = one acoustic period of every system from rest"),
     "c5_sweep": ("c5_sweep: the centre 128 x 128 window of the 1024 x 1024 amplitude (0.5-2 bar, linear) x frequency "
                  "(20-200 kHz, log) grid of N = 32 line systems (d = 150 um, R_E ~ U(2,8) um seed 1), 8 periods with the "
                  "first 4 discarded (--sweep-periods, --sweep-discard); plain solver on every point vs the surrogate-"
@@ -92,6 +96,7 @@ WORKLOADS = {
 
 
 args_c1_factored = True
+args_ring_full = False
 
 
 # periods per bench step and the period before which accessories are reset
@@ -108,6 +113,11 @@ def make_ensemble(name, world=1):
         return W.c2_ensemble(n_systems=16384 * world, n_periods=1, reset_at=-1)
     if name == "c3r_period1":
         return W.c3_radii_ensemble(n_systems=4096 * world, n_periods=1, reset_at=-1)
+    if name == "ring_period1":
+        ens = W.ring_ensemble(n_systems=1024 * world, n_units=128, band_width=1)
+        if args_ring_full:
+            ens.band_width = 0   # the same banded matrices through the full-matrix operator
+        return ens
     return W.c3_ensemble(n_systems=4096 * world, n_periods=1, reset_at=-1)
 
 
@@ -138,6 +148,8 @@ def parse():
                     help="c1_period1 coupling input: the symmetric line geometry 1/d shared by the launch with unit "
                          "factors R^-2, R^3 (default; the same matrix R_j^3/(R_i^2 d_ij) as a product) or the "
                          "reference-format matrix itself")
+    ap.add_argument("--ring-full", action="store_true",
+                    help="ring_period1: solve the banded matrices through the full-matrix operator")
     ap.add_argument("--autotune", type=int, default=1, choices=[0, 1],
                     help="1: pick launch shapes with bes_autotune before the warm-up (untimed)")
     ap.add_argument("--warps-per-system", type=int, default=0, choices=[0, 1],
@@ -289,8 +301,9 @@ def run_b200(args, rank, world, local):
     V = S.ListOfVariables
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    global args_c1_factored
+    global args_c1_factored, args_ring_full
     args_c1_factored = args.c1_format == "geometry"
+    args_ring_full = args.ring_full
     ens_all = make_ensemble(args.workload, world)
     if 0 < args.systems < ens_all.n_systems:
         ens_all = ens_all.subset(list(range(0, ens_all.n_systems, ens_all.n_systems // args.systems))[:args.systems])
@@ -415,6 +428,7 @@ def run_b200(args, rank, world, local):
                    "units_per_system": int(ens.units[0]) if len(set(ens.units.tolist())) == 1 else "mixed",
                    "total_units": ens.total_units,
                    "periods_per_step": n_per,
+                   "band_width": int(ens_all.band_width),
                    "coupling_input": ("shared symmetric geometry G = 1/d with unit factors R^-2, R^3"
                                       if ens.coupling_row_scale is not None else "per-ensemble matrix as given"),
                    "warps_per_system": "one" if args.warps_per_system else "2 or 4 above 32 units",

@@ -372,6 +372,7 @@ DeviceProblem make_problem(bes_solver* h) {
     P.status = (int32_t*)h->buf[B_STATUS].d;
     P.uacc_reset = h->d_uacc_reset;
     P.iuacc_reset = h->d_iuacc_reset;
+    P.band_width = h->cbw;
     return P;
 }
 
@@ -383,7 +384,7 @@ struct ClassLaunch {
 /* launch shape of one class (no stream work: safe before a capture) */
 bes_status plan_shape(bes_solver* h, int cls, int warps_per_system, int requested_wpb, ClassLaunch* L) {
     const bes::Variant v = bes::class_variant(cls, h->class0_all32, h->shared_coupling && h->class_shared[cls],
-                                         warps_per_system, h->class_symmetric[cls], h->bicg_recurrence);
+                                         warps_per_system, h->class_symmetric[cls], h->bicg_recurrence, h->cbw);
     const int count = h->class_count[cls];
     if (bes::max_warps_per_block(v) < v.G)
         return fail(h, BES_ERR_CUDA, "solver kernel variant (U=%d, G=%d) does not fit in shared memory", v.U, v.G);
@@ -1424,7 +1425,7 @@ bes_status bes_autotune(bes_solver* h, int32_t n_periods, int64_t step_cap, bes_
         for (int wps = 0; wps <= (cls == 0 ? 0 : 1) && !st; wps++) {
             const bes::Variant v = bes::class_variant(cls, h->class0_all32,
                                                       h->shared_coupling && h->class_shared[cls], wps,
-                                                      h->class_symmetric[cls], h->bicg_recurrence);
+                                                      h->class_symmetric[cls], h->bicg_recurrence, h->cbw);
             const int cap = bes::max_warps_per_block(v);
             for (int wpb = v.G; wpb <= cap && !st; wpb *= 2) {
                 ClassLaunch L;

@@ -74,6 +74,8 @@ struct DeviceProblem {
     int32_t max_accessory_index;
     int32_t n_sections;              /* Poincare sections stored per call */
     double* poincare;                /* [n_sections][total_units] state component 0 at the end of each period */
+    int32_t band_width;              /* banded coupling storage (CBW > 0): the banded kernel variant's band */
+    int32_t pad;
 };
 
 }  // namespace bes

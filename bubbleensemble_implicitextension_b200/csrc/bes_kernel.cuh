@@ -119,6 +119,22 @@ struct SharedCSmem {
     static_assert(LDC % 2 == 0 && C_DOUBLES % 2 == 0 && WARP_DOUBLES % 2 == 0, "16-byte alignment");
 };
 
+/* Shared-memory layout of the banded variant (RHS = 7, one unit per lane, G
+ * warps, NMAX = 32 G units): per system the staged band of its coupling
+ * matrix Cb[d][i] = C[i][(i + d - bw) mod N] and the operator by diagonal
+ * Wb[d][i], ND = min(2 bw + 1, NMAX) diagonals each, then the six broadcast
+ * vectors, the group's exchange buffers, the system-scope arrays and the unit
+ * parameters.  The band width is a run-time value, so is the layout. */
+template <int G>
+struct BandSmem {
+    static constexpr int NMAX = 32 * G;
+    static constexpr int XCH_DOUBLES = G > 1 ? 2 * XCH_BUF : 0;
+    __host__ __device__ static constexpr int diagonals(int bw) { return 2 * bw + 1 < NMAX ? 2 * bw + 1 : NMAX; }
+    __host__ __device__ static constexpr int doubles(int bw) {
+        return (2 * diagonals(bw) * NMAX + 6 * NMAX + XCH_DOUBLES + NSPa + NSAa + NISAa + NMAX * NUPa + 31) / 32 * 32;
+    }
+};
+
 /* halving-tree sum S(L, i) = S(2L, i) + S(2L, i + L), S(P, i) = leaf(i) */
 template <int L, int P>
 struct TreeSum {
@@ -1045,6 +1061,93 @@ __device__ __forceinline__ int coupled_rhs_regsym(const Sys<1>& S, const DeviceP
     return done;
 }
 
+/* ---------------------------------------------------------------------------
+ * Coupled right-hand side for banded coupling storage (RHS = 7; the
+ * reference's CBW modes, Steppers.cuh:586-641, whose implicit products read
+ * full storage, :660,692): only the wrapping band of nd = min(2 bw + 1, N)
+ * diagonals j = i + d - bw (mod N) couples, so every product costs O(N nd)
+ * instead of O(N^2).  Lane i holds unit i; the system's band Cb[d][i] was
+ * staged at the start of the system, the operator Wb[d][i] = (rD_i C_ij) X1sq_j
+ * is formed per right-hand side, A v sums Wb[d][i] v[j] over d and A^T vt sums
+ * Wb[d][k] vt[k] over k = i + bw - d (mod N), each as four chains over d
+ * (d mod 4) combined (s0 + s1) + (s2 + s3) -- the oracle's banded association. */
+template <int G, int REC>
+__device__ __forceinline__ int coupled_rhs_band(const Sys<1, G>& S, const DeviceProblem& P, double T,
+                                                double (&Xs)[1][UD], double (&F)[1][UD], double (&ua)[1][NUAa],
+                                                int (&iua)[1][NIUAa], bool& capped) {
+    constexpr int NMAX = 32 * G;
+    const int N = S.N;
+    const int bw = P.band_width;
+    const int ND = BandSmem<G>::diagonals(bw);
+    const int nd = ND < N ? ND : N;
+    const int i = S.unit(0);
+    const bool valid = i < N;
+    const double* Cb = S.W;
+    double* Wb = S.W + (size_t)ND * NMAX;
+    /* first column of unit i's band and first row of its transposed band */
+    const int j0 = valid ? ((i - bw) % N + N) % N : 0;
+    const int k0 = valid ? ((i + bw) % N + N) % N : 0;
+    double xu = 0.0, rd = 0.0;
+    grp_sync(S);
+    if (valid) {
+        double Fl[UD], cpt, cpf;
+        CoupledSystems_PerBlock_OdeFunction<double>(S.sid, i, Fl, Xs[0], T, S.upsh + i * NUPa, S.sPAR, S.gPAR,
+                                                    S.igPAR, ua[0], iua[0], S.sACC, S.isACC, &cpt, &cpf);
+#pragma unroll
+        for (int k = 0; k < UD; k++) F[0][k] = Fl[k];
+        xu = Fl[IC];
+        rd = cpf;
+        S.vcpt[i] = cpt;
+        S.vx1[i] = Xs[0][0] * Xs[0][0];
+        S.vxu[i] = Fl[IC];
+    } else {
+#pragma unroll
+        for (int k = 0; k < UD; k++) F[0][k] = 0.0;
+    }
+    grp_sync(S);
+    double r = 0.0;
+    if (valid) {
+        double bs[4] = {0.0, 0.0, 0.0, 0.0}, as[4] = {0.0, 0.0, 0.0, 0.0};
+        int j = j0;
+        for (int d = 0; d < nd; d++) {
+            const double c = Cb[d * NMAX + i];
+            const double x1 = S.vx1[j];
+            bs[d & 3] = fma(c, S.vcpt[j], bs[d & 3]);
+            as[d & 3] = fma(c * x1, S.vxu[j], as[d & 3]);
+            Wb[d * NMAX + i] = (rd * c) * x1;
+            j = j + 1 == N ? 0 : j + 1;
+        }
+        const double b = fma(rd, (bs[0] + bs[1]) + (bs[2] + bs[3]), xu);
+        const double ax = fma(rd, (as[0] + as[1]) + (as[2] + as[3]), xu);
+        r = b - ax;
+    }
+    auto apply = [&](const double (&v)[1], const double (&vt)[1], double (&qo)[1], double (&qto)[1]) {
+        grp_sync(S);
+        S.vp[i] = v[0];
+        S.vpt[i] = vt[0];
+        grp_sync(S);
+        double q = 0.0, qt = 0.0;
+        if (valid) {
+            double qs[4] = {0.0, 0.0, 0.0, 0.0}, ts[4] = {0.0, 0.0, 0.0, 0.0};
+            int j = j0, kk = k0;
+            for (int d = 0; d < nd; d++) {
+                qs[d & 3] = fma(Wb[d * NMAX + i], S.vp[j], qs[d & 3]);
+                ts[d & 3] = fma(Wb[d * NMAX + kk], S.vpt[kk], ts[d & 3]);
+                j = j + 1 == N ? 0 : j + 1;
+                kk = kk == 0 ? N - 1 : kk - 1;
+            }
+            q = v[0] + ((qs[0] + qs[1]) + (qs[2] + qs[3]));
+            qt = vt[0] + ((ts[0] + ts[1]) + (ts[2] + ts[3]));
+        }
+        qo[0] = q;
+        qto[0] = qt;
+    };
+    double rr[1] = {r}, xx[1] = {xu};
+    const int done = bicg_iterate<1, G, REC>(S, P, rr, xx, apply, capped);
+    F[0][IC] = xx[0];
+    return done;
+}
+
 /* the right-hand side a kernel variant uses */
 template <int U, int RHS, int G, int REC>
 __device__ __forceinline__ int rhs_eval(const Sys<U, G>& S, const DeviceProblem& P, double T, double (&Xs)[U][UD],
@@ -1058,6 +1161,9 @@ __device__ __forceinline__ int rhs_eval(const Sys<U, G>& S, const DeviceProblem&
     } else if constexpr (RHS == 5 || RHS == 6) {
         static_assert(U == 1 && G == 1, "the register-resident operator needs one unit per lane");
         return coupled_rhs_regsym<RHS == 6 ? 32 : 0, REC>(S, P, T, Xs, F, ua, iua, ra, cb, grow, capped);
+    } else if constexpr (RHS == 7) {
+        static_assert(U == 1, "the banded operator runs one unit per lane");
+        return coupled_rhs_band<G, REC>(S, P, T, Xs, F, ua, iua, capped);
     } else {
         static_assert(U == 1, "the register-resident operator needs one unit per lane");
         return coupled_rhs_regw<RHS == 2 ? 32 : 0, REC>(S, P, T, Xs, F, up, ua, iua, capped);
@@ -1575,7 +1681,7 @@ __device__ __forceinline__ void analysis_period_end(const Sys<U, G>& S, const De
  * exchanges the group's values through shared memory and a named barrier per
  * system slot (barrier 0 is left to __syncthreads). */
 template <int U, int RHS, int G, int REC>
-__global__ void __launch_bounds__(RHS == 3 || RHS == 4 || G > 1 ? 256 : 128, 1) bes_ensemble_kernel(DeviceProblem P) {
+__global__ void __launch_bounds__(RHS == 3 || RHS == 4 || RHS == 7 || G > 1 ? 256 : 128, 1) bes_ensemble_kernel(DeviceProblem P) {
     static_assert(G == 1 || U == 1, "multi-warp systems run one unit per lane");
     static_assert(G == 1 || (RHS != 1 && RHS != 2 && RHS != 5 && RHS != 6),
                   "the register-resident operators are single-warp");
@@ -1611,6 +1717,21 @@ __global__ void __launch_bounds__(RHS == 3 || RHS == 4 || G > 1 ? 256 : 128, 1) 
         S.vxu = base + 4 * NM;
         S.vrd = nullptr;
         S.xch = base + 5 * NM;
+        S.sPAR = S.xch + SM::XCH_DOUBLES;
+        S.upsh = S.sPAR + NSPa + NSAa + NISAa;
+    } else if constexpr (RHS == 7) {
+        using SM = BandSmem<G>;
+        constexpr int NM = SM::NMAX;
+        const int ND = SM::diagonals(P.band_width);
+        double* base = smem + (size_t)slot * SM::doubles(P.band_width);
+        S.W = base;                                   /* Cb, then Wb */
+        S.vp = base + 2 * (size_t)ND * NM;
+        S.vpt = S.vp + NM;
+        S.vcpt = S.vpt + NM;
+        S.vx1 = S.vcpt + NM;
+        S.vxu = S.vx1 + NM;
+        S.vrd = S.vxu + NM;
+        S.xch = S.vrd + NM;
         S.sPAR = S.xch + SM::XCH_DOUBLES;
         S.upsh = S.sPAR + NSPa + NSAa + NISAa;
     } else {
@@ -1687,6 +1808,17 @@ __global__ void __launch_bounds__(RHS == 3 || RHS == 4 || G > 1 ? 256 : 128, 1) 
 #pragma unroll
             for (int j = 0; j < 32; j++)
                 L.grow[j] = (lane < S.N && j < S.N) ? __ldg(S.C + lane + (int64_t)j * S.N) : 0.0;
+        }
+        if constexpr (RHS == 7) {
+            /* stage the system's band: Cb[d][i] = C[i][(i + d - bw) mod N] */
+            constexpr int NM = BandSmem<G>::NMAX;
+            const int ND = BandSmem<G>::diagonals(P.band_width);
+            const int nd = ND < S.N ? ND : S.N;
+            for (int idx = 32 * S.wis + lane; idx < nd * NM; idx += 32 * G) {
+                const int d = idx / NM, r = idx % NM;
+                const int c = ((r + d - P.band_width) % S.N + S.N) % S.N;
+                S.W[idx] = r < S.N ? __ldg(S.C + r + (int64_t)c * S.N) : 0.0;
+            }
         }
         if constexpr (RHS == 1 || RHS == 2) {
             /* stage the system's coupling matrix, zero-padded to 32 x 33 */

@@ -6,4 +6,5 @@ namespace bes {
 BES_KERNEL_VARIANT(1, 0, 4, 1, BES_SMEM_WARP(1, 4))
 BES_KERNEL_VARIANT(1, 3, 4, 1, BES_SMEM_SHARED(1, 4))
 BES_KERNEL_VARIANT(1, 4, 4, 1, BES_SMEM_SHARED(1, 4))
+BES_KERNEL_VARIANT(1, 7, 4, 1, BES_SMEM_BAND(4))
 }  // namespace bes

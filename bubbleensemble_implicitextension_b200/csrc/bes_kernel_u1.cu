@@ -7,4 +7,5 @@ BES_KERNEL_VARIANT(1, 1, 1, 0, BES_SMEM_WARP(1, 1))
 BES_KERNEL_VARIANT(1, 2, 1, 0, BES_SMEM_WARP(1, 1))
 BES_KERNEL_VARIANT(1, 5, 1, 0, BES_SMEM_WARP(1, 1))
 BES_KERNEL_VARIANT(1, 6, 1, 0, BES_SMEM_WARP(1, 1))
+BES_KERNEL_VARIANT(1, 7, 1, 0, BES_SMEM_BAND(1))
 }  // namespace bes

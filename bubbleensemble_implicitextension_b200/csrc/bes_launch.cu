@@ -33,6 +33,9 @@ bool dispatch_rec(Variant v, F&& f) {
         case 132: f(Tag<1, 3, 2, REC>{}); return true;
         case 104: f(Tag<1, 0, 4, REC>{}); return true;
         case 134: f(Tag<1, 3, 4, REC>{}); return true;
+        case 171: f(Tag<1, 7, 1, REC>{}); return true;
+        case 172: f(Tag<1, 7, 2, REC>{}); return true;
+        case 174: f(Tag<1, 7, 4, REC>{}); return true;
         default: return false;
     }
 }
@@ -53,13 +56,13 @@ bool variant_exists(Variant v) {
 
 size_t cta_smem_bytes(Variant v, int warps) {
     size_t r = 0;
-    dispatch(v, [&](auto t) { using T = decltype(t); r = cta_smem_t<T::U, T::RHS, T::G, T::REC>(warps); });
+    dispatch(v, [&](auto t) { using T = decltype(t); r = cta_smem_t<T::U, T::RHS, T::G, T::REC>(warps, v.band); });
     return r;
 }
 
 int max_warps_per_block(Variant v) {
     /* the kernels' launch bounds: 256 threads with RHS 3 or G > 1, else 128 */
-    const int cap = (v.rhs == 3 || v.rhs == 4 || v.G > 1) ? 8 : 4;
+    const int cap = (v.rhs == 3 || v.rhs == 4 || v.rhs == 7 || v.G > 1) ? 8 : 4;
     int w = 0;
     while (w + v.G <= cap && cta_smem_bytes(v, w + v.G) <= 227 * 1024) w += v.G;
     return w;
@@ -67,7 +70,7 @@ int max_warps_per_block(Variant v) {
 
 cudaError_t occupancy(Variant v, int warps, int* ctas_per_sm) {
     cudaError_t e = cudaErrorInvalidValue;
-    dispatch(v, [&](auto t) { using T = decltype(t); e = occupancy_t<T::U, T::RHS, T::G, T::REC>(warps, ctas_per_sm); });
+    dispatch(v, [&](auto t) { using T = decltype(t); e = occupancy_t<T::U, T::RHS, T::G, T::REC>(warps, v.band, ctas_per_sm); });
     return e;
 }
 
@@ -81,14 +84,19 @@ cudaError_t launch(Variant v, const DeviceProblem& P, int grid, int warps, cudaS
  * (rhs 2: every system has exactly 32 units); larger N runs one unit per lane
  * on 2 or 4 warps (or 2 or 4 units per lane on one warp) with W in shared
  * memory, or one staged copy of a matrix shared by the whole class when the
- * caller asked for shared coupling matrices (SharedCouplingMatrices). */
-Variant class_variant(int cls, bool all32, bool shared, int warps_per_system, bool symmetric, int rec) {
+ * caller asked for shared coupling matrices (SharedCouplingMatrices).  With
+ * banded coupling storage (band > 0) every class whose matrix is not staged
+ * as a shared symmetric (N <= 32) or shared (N > 32) matrix runs the banded
+ * operator, one unit per lane on 1, 2 or 4 warps. */
+Variant class_variant(int cls, bool all32, bool shared, int warps_per_system, bool symmetric, int rec, int band) {
     if (cls == 0) {
         if (shared && symmetric) return Variant{1, all32 ? 6 : 5, 1, rec};   /* row of G in registers */
+        if (band > 0) return Variant{1, 7, 1, rec, band};
         return Variant{1, all32 ? 2 : 1, 1, rec};
     }
-    const int rhs = shared ? (symmetric ? 4 : 3) : 0;
     const int width = cls == 1 ? 2 : 4;
+    if (!shared && band > 0) return Variant{1, 7, width, rec, band};   /* banded storage: one unit per lane */
+    const int rhs = shared ? (symmetric ? 4 : 3) : 0;
     if (warps_per_system == 1) return Variant{width, rhs, 1, rec};
     return Variant{1, rhs, width, rec};
 }

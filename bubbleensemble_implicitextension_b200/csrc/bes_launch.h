@@ -9,7 +9,8 @@
  * per CTA (64 or 128 units), RHS 4 is RHS 3 for a symmetric shared matrix
  * (both BiCG products as row sums from one shared-memory read); RHS 5 / 6
  * (U = G = 1, N <= 32) keep a row of a shared symmetric matrix in registers
- * (6: every system has 32 units).  Every variant exists with both BiCG
+ * (6: every system has 32 units); RHS 7 (U = 1) keeps only the wrapping
+ * band of banded coupling storage (CBW > 0).  Every variant exists with both BiCG
  * recurrences (REC 0: the reference's; 1: the single-reduction form). */
 #ifndef BES_LAUNCH_H
 #define BES_LAUNCH_H
@@ -26,6 +27,7 @@ namespace bes {
 struct Variant {
     int U, rhs, G;
     int rec = 0;
+    int band = 0;   /* band width of the banded variant (RHS 7) */
 };
 
 /* is (U, RHS, G) one of the built variants */
@@ -43,15 +45,16 @@ cudaError_t launch(Variant v, const DeviceProblem& P, int grid, int warps, cudaS
  * every system of the launch has 32 units; shared: the launch shares one
  * coupling matrix; warps_per_system 1 keeps every system on one warp; rec:
  * the BiCG recurrence */
-Variant class_variant(int cls, bool all32, bool shared, int warps_per_system, bool symmetric = false, int rec = 0);
+Variant class_variant(int cls, bool all32, bool shared, int warps_per_system, bool symmetric = false, int rec = 0,
+                      int band = 0);
 /* warps per CTA for `count` systems of variant v (requested > 0: that many,
  * clamped to what the variant allows and rounded down to a multiple of G) */
 int class_warps_per_block(Variant v, int count, int sm_count, int requested);
 
 template <int U, int RHS, int G, int REC>
-size_t cta_smem_t(int warps);
+size_t cta_smem_t(int warps, int band);
 template <int U, int RHS, int G, int REC>
-cudaError_t occupancy_t(int warps, int* ctas_per_sm);
+cudaError_t occupancy_t(int warps, int band, int* ctas_per_sm);
 template <int U, int RHS, int G, int REC>
 cudaError_t launch_t(const DeviceProblem& P, int grid, int warps, cudaStream_t stream);
 

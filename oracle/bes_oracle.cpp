@@ -139,13 +139,15 @@ int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
                 const double* ra = nullptr, const double* cb = nullptr, bool symmetric = false, int variant = 0,
                 int bw = 0) {
     const int N = w.N;
-    /* banded association (bw > 0, 2 bw + 1 < N): only the wrapping band
-     * j = i + d - bw (mod N), d = 0 .. 2 bw, of C is read, with four chains over
-     * d (d mod 4); W is kept by diagonal, Wb[d][i] = W[i][j(i, d)], and the
-     * transposed product of unit i sums Wb[d][k] vt[k] over k = i + bw - d (mod N) */
-    const bool band = bw > 0 && 2 * bw + 1 < N && !shared_assoc;
-    const int nd = 2 * bw + 1;
-    auto jband = [&](int i, int d) { int j = i + d - bw; if (j < 0) j += N; if (j >= N) j -= N; return j; };
+    /* banded association (banded storage, bw > 0, and no shared-matrix
+     * association): only the wrapping band j = i + d - bw (mod N),
+     * d = 0 .. nd - 1, nd = min(2 bw + 1, N), of C is read (with nd = N every
+     * column exactly once), with four chains over d (d mod 4); W is kept by
+     * diagonal, Wb[d][i] = W[i][j(i, d)], and the transposed product of unit i
+     * sums Wb[d][k] vt[k] over k = i + bw - d (mod N) */
+    const bool band = bw > 0 && !shared_assoc;
+    const int nd = std::min(2 * bw + 1, N);
+    auto jband = [&](int i, int d) { return (((i + d - bw) % N) + N) % N; };
     auto band_sum4 = [&](auto term) {
         double c[4] = {0.0, 0.0, 0.0, 0.0};
         for (int d = 0; d < nd; d++) term(d, c[d & 3]);
@@ -208,7 +210,7 @@ int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
             for (int i = 0; i < N; i++) {
                 q[i] = v[i] + band_sum4([&](int d, double& acc) { acc = fma(w.W[i + (long)d * N], v[jband(i, d)], acc); });
                 qt[i] = vt[i] + band_sum4([&](int d, double& acc) {
-                    const int k = jband(i, 2 * bw - d);   /* k = i + bw - d */
+                    const int k = (((i + bw - d) % N) + N) % N;
                     acc = fma(w.W[k + (long)d * N], vt[k], acc);
                 });
             }

@@ -1,9 +1,11 @@
 """Banded and circular coupling storage (the reference's CBW / CCI modes,
 Interface.cuh:1010-1070, ExplicitRungeKutta_Steppers.cuh:586-641): elements set
-through SetHost in full-matrix coordinates give exactly the run with the full
-matrix those formats describe, which the implicit solve then uses (the
-reference's implicit products read full storage in every mode,
-Steppers.cuh:660,692)."""
+through SetHost in full-matrix coordinates describe the full matrix of those
+formats (the reference's implicit products read full storage in every mode,
+Steppers.cuh:660,692).  With CBW > 0 the solve runs the banded operator
+(only the 2 CBW + 1 diagonals); with CBW = 1 each row has at most two nonzero
+terms, so its sums equal the full matrix's bit for bit, which is what these
+tests check (tests/test_gpu_banded.py covers wider bands against the oracle)."""
 import numpy as np
 import pytest
 
