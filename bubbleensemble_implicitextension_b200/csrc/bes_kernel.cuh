@@ -504,7 +504,8 @@ __device__ __forceinline__ int bicg_iterate(const Sys<U, G>& S, const DeviceProb
             apply(p, pt, q, qt);
 #pragma unroll
             for (int m = 0; m < U; m++) prod[m] = pt[m] * q[m];
-            const double alpha = rho1 / grp_tree_sum<U, G>(S, prod);
+            const double sig = grp_tree_sum<U, G>(S, prod);
+            const double alpha = math::div_known(rho1, sig, math::recip_estimate(sig));   /* = rho1 / sig */
 #pragma unroll
             for (int m = 0; m < U; m++) {
                 x[m] = fma(alpha, p[m], x[m]);
@@ -551,7 +552,7 @@ __device__ __forceinline__ int bicg_iterate(const Sys<U, G>& S, const DeviceProb
                     qt[m] = fma(beta, qt[m], wt[m]);
                 }
             }
-            const double alpha = rho / sigma;
+            const double alpha = math::div_known(rho, sigma, math::recip_estimate(sigma));   /* = rho / sigma */
             rho_prev = rho;
             y_prev = math::recip_estimate(rho);
 #pragma unroll

@@ -109,3 +109,25 @@ def gather_results(local: Dict[str, np.ndarray], rank: int, world: int) -> Optio
         axis = -1 if k in UNIT_KEYS else 0
         out[k] = np.concatenate([p[k] for p in parts], axis=axis)
     return out
+
+
+def sharded_points_solve(solve: Callable[[np.ndarray, np.ndarray], np.ndarray], rank: int, world: int,
+                         cost: Optional[Callable[[np.ndarray, np.ndarray], np.ndarray]] = None):
+    """A sweep's solve callback split over the ranks: the requested points are cut
+    into contiguous shares (of equal count, or of equal estimated cost when
+    `cost(pa, f)` gives one per point), each rank integrates its share with
+    `solve`, and the outputs are all-gathered so that every rank returns the
+    full [n, k] array.  Every rank must call it with the same points in the
+    same order (the sweep screener is deterministic, so it does)."""
+    if world == 1:
+        return solve
+
+    def run(pa_pts: np.ndarray, f_pts: np.ndarray) -> np.ndarray:
+        n = len(pa_pts)
+        b = cost_bounds(cost(pa_pts, f_pts), world) if cost is not None else even_bounds(n, world)
+        lo, hi = int(b[rank]), int(b[rank + 1])
+        mine = solve(pa_pts[lo:hi], f_pts[lo:hi]) if hi > lo else None
+        parts = _all_gather_object(None if mine is None else np.asarray(mine), world)
+        return np.concatenate([p for p in parts if p is not None], axis=0)
+
+    return run

@@ -133,3 +133,57 @@ def test_cost_bounds_properties():
             if n >= world:
                 shares = [c[b[r]:b[r + 1]].sum() for r in range(world)]
                 assert max(shares) - c.sum() / world <= c.max() + 1e-9
+
+
+def _sweep_worker(rank, world, port, out):
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank), MASTER_ADDR="127.0.0.1",
+                      MASTER_PORT=str(port))
+    import datetime
+
+    import torch.distributed as dist
+
+    from bubbleensemble_implicitextension_b200 import sharding as SH
+    from bubbleensemble_implicitextension_b200 import surrogate as SG
+    from tests.test_sweep_screen import _Net, _grid, _map
+
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+    calls = []
+
+    def solve_local(pp, ff):
+        calls.append(len(pp))
+        return _map(pp, ff, True)
+
+    pa, f = _grid()
+    solve = SH.sharded_points_solve(solve_local, rank, world)
+    res = SG.screen_sweep_lattice(_Net(), pa, f, np.full(32, 5.0), solve, stride=4, cell_spread=0.5,
+                                  cell_disagreement=0.05, audit_fraction=0.05, seed=2)
+    out[rank] = (res.map, res.integrated, sum(calls))
+    dist.destroy_process_group()
+
+
+@pytest.mark.timeout(300)
+def test_sharded_sweep_screen_equals_single_rank():
+    """The sweep screener with its solves split over two gloo ranks: both ranks end
+    with the single-rank map, and the points were shared between them."""
+    from bubbleensemble_implicitextension_b200 import surrogate as SG
+    from tests.test_sweep_screen import _Net, _grid, _map
+
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        out = mgr.dict()
+        port = _free_port()
+        procs = [ctx.Process(target=_sweep_worker, args=(r, 2, port, out)) for r in range(2)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(240)
+            assert p.exitcode == 0
+        res = dict(out)
+    pa, f = _grid()
+    single = SG.screen_sweep_lattice(_Net(), pa, f, np.full(32, 5.0), lambda pp, ff: _map(pp, ff, True), stride=4,
+                                     cell_spread=0.5, cell_disagreement=0.05, audit_fraction=0.05, seed=2)
+    for r in range(2):
+        np.testing.assert_array_equal(res[r][0], single.map)
+        np.testing.assert_array_equal(res[r][1], single.integrated)
+    assert res[0][2] + res[1][2] == int(single.integrated.sum())   # each point integrated once, on one rank
+    assert res[0][2] > 0 and res[1][2] > 0
