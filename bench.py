@@ -443,6 +443,10 @@ def run_b200(args, rank, world, local):
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None,
                      "traffic": read_traffic() if args.workload == "c1_period1" else None,
+                     "traffic_source": ("DRAM bytes of one launch from the committed ncu capture "
+                                        "profiles/bes_ensemble_kernel_c1_period1.md (a 32-system small case scaled by "
+                                        "the systems processed), not measured in this run"
+                                        if args.workload == "c1_period1" else None),
                      "peak_source": "measured live: bes_measure_fp64_peak FMA-throughput loop (no FP64 figure in "
                                     "MEASURED_PEAKS.json)",
                      "flops_per_launch": flops, "kernel": "bes::bes_ensemble_kernel (all classes of the launch plan)"},
@@ -458,9 +462,51 @@ def run_b200(args, rank, world, local):
                      "completed_system_periods_per_s": float(((gathered["status"] & 4) == 0).sum() * n_per * args.steps
                                                              / (max_ms * 1e-3))},
     }
+    if world == 1 and args.workload == "c1_period1" and args.c1_format == "geometry":
+        # like for like with the reference arm: the same ensemble with the reference-format matrix as input
+        line["reference_format_input"] = reference_format_steps(args, local, flush)
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(ens, args.cpu_sample_systems)
     return line
+
+
+def reference_format_steps(args, local, flush):
+    """c1_period1 with the coupling given as the reference-format matrix C_ij = R_j^3 / (R_i^2 d_ij) (the
+    reference arm's input): device-resident throughput over the same number of timed steps."""
+    import torch
+
+    from bubbleensemble_implicitextension_b200 import solver as S
+    from bubbleensemble_implicitextension_b200 import workloads as W
+    V = S.ListOfVariables
+    ens = W.c1_ensemble(n_periods=1, reset_at=-1, factored=False)
+    ens.max_steps_per_period = 50_000
+    ps = ens.make_solver(device=local)
+    try:
+        ps.SolverOption(S.ListOfSolverOptions.BiCGRecurrence, args.bicg_recurrence)
+        stream = torch.cuda.current_stream()
+        ps.set_stream(stream.cuda_stream)
+        ps.SynchroniseFromHostToDevice(V.All)
+        torch.cuda.synchronize()
+        if args.autotune:
+            ps.autotune(n_periods=1, step_cap=2000)
+        times = []
+        for it in range(args.warmup + args.steps):
+            ps.SynchroniseFromHostToDevice(V.ActualState)
+            ps.SynchroniseFromHostToDevice(V.UnitAccessories)
+            ps.SynchroniseFromHostToDevice(V.IntegerUnitAccessories)
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ps.solve_periods(1, -1)
+            e1.record(stream)
+            e1.synchronize()
+            if it >= args.warmup:
+                times.append(e0.elapsed_time(e1))
+    finally:
+        ps.close()
+    ms = float(np.mean(times))
+    return {"value": ens.n_systems / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "steps": args.steps,
+            "input": "the reference-format matrix R_j^3 / (R_i^2 d_ij) per system, as the reference arm takes it"}
 
 
 def solve_counters(ens, device, bicg_recurrence):
