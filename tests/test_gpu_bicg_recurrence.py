@@ -63,7 +63,7 @@ def test_dense_output_and_cap_match_oracle(gpu, oracle_lib):
     assert (got["status"] & 16).any(), "the cap of 3 iterations was never reached"
 
 
-@pytest.mark.parametrize("name", list(cases.CASES))
+@pytest.mark.parametrize("name", cases.AVAILABLE)
 def test_matches_reference_golden(gpu, name):
     ens, run = cases.build(name)
     got = run_gpu(ens, n_periods=run["n_periods"], reset_at=run["reset_at"], ndo=run.get("ndo", 0),

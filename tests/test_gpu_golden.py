@@ -8,7 +8,7 @@ from tests.helpers import run_gpu
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("name", list(cases.CASES))
+@pytest.mark.parametrize("name", cases.AVAILABLE)
 def test_kernel_matches_reference_golden(name, gpu):
     ens, run = cases.build(name)
     got = run_gpu(ens, n_periods=run["n_periods"], reset_at=run["reset_at"], ndo=run.get("ndo", 0),

@@ -10,15 +10,16 @@ from tests import golden_compare
 from tests.golden import cases
 
 
-@pytest.mark.parametrize("name", list(cases.CASES))
+@pytest.mark.parametrize("name", cases.AVAILABLE)
 def test_oracle_matches_reference_golden(name, oracle_lib):
-    ens, run = cases.build(name)
+    sub = cases.CPU_SUBSET.get(name)
+    ens, run = cases.build(name, subset=sub)
     got = oracle_lib.run(ens, n_periods=run["n_periods"], reset_at=run["reset_at"], ndo=run.get("ndo", 0),
                          do_min_dt=run.get("do_min_dt", 0.0), do_save_frequency=run.get("do_save_frequency", 1))
-    golden_compare.check(name, got)
+    golden_compare.check(name, got, subset=sub)
 
 
 def test_golden_fixtures_present():
-    for name in cases.CASES:
+    for name in cases.AVAILABLE:
         g, case = golden_compare.load(name)
         assert case["name"] == name and "state" in g and "uacc" in g
