@@ -88,7 +88,7 @@ struct WarpSmem {
     static constexpr int LDW = NMAX + 1;
     static constexpr int W_DOUBLES = NMAX * LDW;
     static constexpr int VEC_DOUBLES = 6 * NMAX;
-    static constexpr int XCH_DOUBLES = G > 1 ? 2 * XCH_BUF : 0; /* two buffers of two values per unit + flags */
+    static constexpr int XCH_DOUBLES = G > 1 ? 2 * XCH_BUF + 8 : 0; /* two buffers of two values per unit, vote words */
     static constexpr int SYS_DOUBLES = NSPa + NSAa + NISAa;  /* ints stored in double slots */
     static constexpr int UP_DOUBLES = U == 1 ? NMAX * NUPa : 0; /* unit parameters (one unit per lane) */
     static constexpr int WT_DOUBLES = U == 1 && G == 1 ? NMAX * LDW : 0;  /* operator W of the register variants */
@@ -111,7 +111,7 @@ struct SharedCSmem {
     static constexpr int NMAX = 32 * U * G;
     static constexpr int LDC = NMAX + 2;
     static constexpr int C_DOUBLES = NMAX * LDC;
-    static constexpr int XCH_DOUBLES = G > 1 ? 2 * XCH_BUF : 0;
+    static constexpr int XCH_DOUBLES = G > 1 ? 2 * XCH_BUF + 8 : 0;
     static constexpr int UP_DOUBLES = U == 1 ? NMAX * NUPa : 0; /* unit parameters (one unit per lane) */
     static constexpr int WARP_DOUBLES = (5 * NMAX + XCH_DOUBLES + NSPa + NSAa + NISAa + UP_DOUBLES + 31) / 32 * 32;
     static constexpr int C_BYTES = C_DOUBLES * 8;
@@ -128,7 +128,7 @@ struct SharedCSmem {
 template <int G>
 struct BandSmem {
     static constexpr int NMAX = 32 * G;
-    static constexpr int XCH_DOUBLES = G > 1 ? 2 * XCH_BUF : 0;
+    static constexpr int XCH_DOUBLES = G > 1 ? 2 * XCH_BUF + 8 : 0;
     __host__ __device__ static constexpr int diagonals(int bw) { return 2 * bw + 1 < NMAX ? 2 * bw + 1 : NMAX; }
     __host__ __device__ static constexpr int doubles(int bw) {
         return (2 * diagonals(bw) * NMAX + 6 * NMAX + XCH_DOUBLES + NSPa + NSAa + NISAa + NMAX * NUPa + 31) / 32 * 32;
@@ -183,6 +183,7 @@ struct Sys {
     double *vp, *vpt, *vcpt, *vx1, *vxu, *vrd;
     double* upsh;      /* unit parameters of the register-operator variant: unit i at upsh[i * NUP] */
     double* xch;       /* the group's exchange buffers (G > 1) */
+    double* flag;      /* the group's exit-vote words, one per warp (G > 1) */
     mutable int xsel;  /* which exchange buffer the next group exchange uses */
     double* sPAR;
     double* sACC;
@@ -418,11 +419,12 @@ __device__ __forceinline__ bool grp_max_below(const Sys<U, G>& S, const double (
     }
 }
 
-/* exit test and two sums in one exchange (multi-warp groups) */
+/* The exit test of a multi-warp group, posted before a barrier: each warp's
+ * votes go to its flag word, the group crosses one barrier, every warp reads
+ * all flags.  The flag words are rewritten only after a later group exchange,
+ * which every reader of the current flags passes after reading them. */
 template <int U, int G>
-__device__ __forceinline__ bool grp_sum2_max_below(const Sys<U, G>& S, const double (&x)[U], const double (&y)[U],
-                                                   const double (&z)[U], double lim, double& ysum, double& zsum) {
-    static_assert(G > 1, "single warps test by votes");
+__device__ __forceinline__ bool grp_flags_max_below(const Sys<U, G>& S, const double (&x)[U], double lim) {
     bool ok = true, seen = false;
 #pragma unroll
     for (int m = 0; m < U; m++) {
@@ -430,23 +432,12 @@ __device__ __forceinline__ bool grp_sum2_max_below(const Sys<U, G>& S, const dou
         seen = seen || !isnan(x[m]);
     }
     const bool wok = __all_sync(FULL, ok), wseen = __any_sync(FULL, seen);
-    double* buf = grp_buffer(S);
-    constexpr int NB = U * G;
-#pragma unroll
-    for (int m = 0; m < U; m++) {
-        buf[(G * m + S.wis) * 32 + S.lane] = y[m];
-        buf[32 * NB + (G * m + S.wis) * 32 + S.lane] = z[m];
-    }
-    if (S.lane == 0) buf[64 * NB + S.wis] = (wok ? 1.0 : 0.0) + (wseen ? 2.0 : 0.0);
+    if (S.lane == 0) S.flag[S.wis] = (wok ? 1.0 : 0.0) + (wseen ? 2.0 : 0.0);
     grp_sync(S);
-    double a[NB], b[NB];
-#pragma unroll
-    for (int k = 0; k < NB; k++) { a[k] = buf[k * 32 + S.lane]; b[k] = buf[32 * NB + k * 32 + S.lane]; }
-    warp_tree_sum2<NB>(a, b, ysum, zsum);
     bool all_ok = true, any_seen = false;
 #pragma unroll
     for (int w = 0; w < G; w++) {
-        const double f = buf[64 * NB + w];
+        const double f = S.flag[w];
         all_ok = all_ok && (f == 1.0 || f == 3.0);
         any_seen = any_seen || f >= 2.0;
     }
@@ -471,9 +462,10 @@ __device__ __forceinline__ bool grp_sum2_max_below(const Sys<U, G>& S, const dou
  * -rho/alpha_prev = -beta sigma_prev each, by the biorthogonality of the
  * residuals).  Same exits as the reference (|rho| < 1e-6 before the first
  * update, max |r| < 1e-6 after each, at most bicg_max_iter updates); a
- * single warp tests by votes right after the update, a group folds the test
- * into the next reduction's exchange (the test sees the same r).  Returns the
- * completed iterations; sets capped when the cap ended the loop. */
+ * single warp tests by votes right after the update, a group posts each warp's
+ * votes before the barrier that opens the next product phase (the test sees
+ * the same r, and no barrier or product is added).  Returns the completed
+ * iterations; sets capped when the cap ended the loop. */
 template <int U, int G, int REC, class Apply>
 __device__ __forceinline__ int bicg_iterate(const Sys<U, G>& S, const DeviceProblem& P, double (&r)[U],
                                             double (&x)[U], Apply&& apply, bool& capped) {
@@ -501,7 +493,7 @@ __device__ __forceinline__ int bicg_iterate(const Sys<U, G>& S, const DeviceProb
                 }
             }
             const double y1 = math::recip_estimate(rho1);   /* becomes y2 at the end of the iteration */
-            apply(p, pt, q, qt);
+            apply(p, pt, q, qt, false);
 #pragma unroll
             for (int m = 0; m < U; m++) prod[m] = pt[m] * q[m];
             const double sig = grp_tree_sum<U, G>(S, prod);
@@ -526,16 +518,22 @@ __device__ __forceinline__ int bicg_iterate(const Sys<U, G>& S, const DeviceProb
         double w[U], wt[U], rw[U];
         double sigma = 0.0, rho_prev = 0.0, y_prev = 0.0;   /* y_prev: reciprocal estimate of rho_prev */
         for (int iter = 1; iter <= P.bicg_max_iter; iter++) {
-            apply(r, rt, w, wt);
+            if constexpr (G > 1) {
+                if (iter > 1) {
+                    /* the exit test of the previous update: every warp posts its vote
+                     * before the barrier the product phase needs anyway */
+                    if (grp_flags_max_below<U, G>(S, ar, 1e-6)) { exited = true; break; }
+                    apply(r, rt, w, wt, true);
+                } else {
+                    apply(r, rt, w, wt, false);
+                }
+            } else {
+                apply(r, rt, w, wt, false);
+            }
 #pragma unroll
             for (int m = 0; m < U; m++) { prod[m] = r[m] * rt[m]; rw[m] = rt[m] * w[m]; }
             double rho, mu;
-            if constexpr (G == 1) {
-                grp_tree_sum2<U, G>(S, prod, rw, rho, mu);
-            } else {
-                if (iter == 1) grp_tree_sum2<U, G>(S, prod, rw, rho, mu);
-                else if (grp_sum2_max_below<U, G>(S, ar, prod, rw, 1e-6, rho, mu)) { exited = true; break; }
-            }
+            grp_tree_sum2<U, G>(S, prod, rw, rho, mu);
             if (iter == 1) {
                 if (fabs(rho) < 1e-6) { exited = true; break; }
 #pragma unroll
@@ -647,8 +645,8 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U, G>& S, const DeviceProbl
         x[m] = xu[m];
     }
     /* q = A v (row sums of W), q~ = A^T vt (column tree of W) */
-    auto apply = [&](const double (&v)[U], const double (&vt)[U], double (&q)[U], double (&qt)[U]) {
-        grp_sync(S);
+    auto apply = [&](const double (&v)[U], const double (&vt)[U], double (&q)[U], double (&qt)[U], bool presynced) {
+        if (!presynced) grp_sync(S);
 #pragma unroll
         for (int m = 0; m < U; m++) {
             const int i = S.unit(m);
@@ -764,8 +762,8 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
     const double2* vp2 = reinterpret_cast<const double2*>(S.vp);
     const double2* vpt2 = reinterpret_cast<const double2*>(S.vpt);
     /* q = A v (row of W in registers), q~ = A^T vt (column of W from shared memory) */
-    auto apply = [&](const double (&v)[1], const double (&vt)[1], double (&qo)[1], double (&qto)[1]) {
-        __syncwarp();
+    auto apply = [&](const double (&v)[1], const double (&vt)[1], double (&qo)[1], double (&qto)[1], bool presynced) {
+        if (!presynced) __syncwarp();
         S.vp[i] = v[0];
         S.vpt[i] = vt[0];
         __syncwarp();
@@ -928,8 +926,8 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const Dev
         x[m] = xu[m];
     }
     /* q = A v = v + rD a (G (b X1sq v)), q~ = A^T vt = vt + b X1sq (G^T (rD a vt)) */
-    auto apply = [&](const double (&v)[U], const double (&vt)[U], double (&q)[U], double (&qt)[U]) {
-        grp_sync(S);
+    auto apply = [&](const double (&v)[U], const double (&vt)[U], double (&q)[U], double (&qt)[U], bool presynced) {
+        if (!presynced) grp_sync(S);
 #pragma unroll
         for (int m = 0; m < U; m++) {
             const int i = S.unit(m);
@@ -1045,8 +1043,8 @@ __device__ __forceinline__ int coupled_rhs_regsym(const Sys<1>& S, const DeviceP
         r = b - ax;
     }
     /* q = A v = v + v_f (G (u v)), q~ = A^T vt = vt + u (G (v_f vt)) with u = b X1sq, v_f = rD a */
-    auto apply = [&](const double (&v)[1], const double (&vt)[1], double (&qo)[1], double (&qto)[1]) {
-        __syncwarp();
+    auto apply = [&](const double (&v)[1], const double (&vt)[1], double (&qo)[1], double (&qto)[1], bool presynced) {
+        if (!presynced) __syncwarp();
         S.vp[i] = x1 * v[0];     /* z  = u v  */
         S.vpt[i] = rd * vt[0];   /* z~ = v_f vt */
         __syncwarp();
@@ -1122,8 +1120,8 @@ __device__ __forceinline__ int coupled_rhs_band(const Sys<1, G>& S, const Device
         const double ax = fma(rd, (as[0] + as[1]) + (as[2] + as[3]), xu);
         r = b - ax;
     }
-    auto apply = [&](const double (&v)[1], const double (&vt)[1], double (&qo)[1], double (&qto)[1]) {
-        grp_sync(S);
+    auto apply = [&](const double (&v)[1], const double (&vt)[1], double (&qo)[1], double (&qto)[1], bool presynced) {
+        if (!presynced) grp_sync(S);
         S.vp[i] = v[0];
         S.vpt[i] = vt[0];
         grp_sync(S);
@@ -1718,6 +1716,7 @@ __global__ void __launch_bounds__(RHS == 3 || RHS == 4 || RHS == 7 || G > 1 ? 25
         S.vxu = base + 4 * NM;
         S.vrd = nullptr;
         S.xch = base + 5 * NM;
+        S.flag = S.xch + 2 * XCH_BUF;
         S.sPAR = S.xch + SM::XCH_DOUBLES;
         S.upsh = S.sPAR + NSPa + NSAa + NISAa;
     } else if constexpr (RHS == 7) {
@@ -1733,6 +1732,7 @@ __global__ void __launch_bounds__(RHS == 3 || RHS == 4 || RHS == 7 || G > 1 ? 25
         S.vxu = S.vx1 + NM;
         S.vrd = S.vxu + NM;
         S.xch = S.vrd + NM;
+        S.flag = S.xch + 2 * XCH_BUF;
         S.sPAR = S.xch + SM::XCH_DOUBLES;
         S.upsh = S.sPAR + NSPa + NSAa + NISAa;
     } else {
@@ -1746,6 +1746,7 @@ __global__ void __launch_bounds__(RHS == 3 || RHS == 4 || RHS == 7 || G > 1 ? 25
         S.vxu = S.vx1 + SM::NMAX;
         S.vrd = S.vxu + SM::NMAX;
         S.xch = S.vrd + SM::NMAX;
+        S.flag = S.xch + 2 * XCH_BUF;
         S.sPAR = S.xch + SM::XCH_DOUBLES;
         S.upsh = S.sPAR + SM::SYS_DOUBLES;
     }
