@@ -467,14 +467,14 @@ __device__ __forceinline__ bool grp_flags_max_below(const Sys<U, G>& S, const do
  * the same r, and no barrier or product is added).  Returns the completed
  * iterations; sets capped when the cap ended the loop. */
 template <int U, int G, int REC, class Apply>
-__device__ __forceinline__ int bicg_iterate(const Sys<U, G>& S, const DeviceProblem& P, double (&r)[U],
-                                            double (&x)[U], Apply&& apply, bool& capped) {
+__device__ __forceinline__ int bicg_iterate(const Sys<U, G>& S, const DeviceProblem& P, const double (&b)[U],
+                                            double (&r)[U], double (&x)[U], Apply&& apply, bool& capped) {
     double rt[U], p[U], pt[U], q[U], qt[U], prod[U], ar[U];
 #pragma unroll
     for (int m = 0; m < U; m++) { rt[m] = r[m]; p[m] = 0.0; pt[m] = 0.0; ar[m] = 0.0; }
     int done = 0;
     bool exited = false;
-    if constexpr (REC == 0) {
+    auto reference_recurrence = [&]() {
 #pragma unroll
         for (int m = 0; m < U; m++) prod[m] = r[m] * rt[m];
         double rho1 = grp_tree_sum<U, G>(S, prod);
@@ -514,7 +514,13 @@ __device__ __forceinline__ int bicg_iterate(const Sys<U, G>& S, const DeviceProb
             if (small) { exited = true; break; }
             rho1 = rho_next;
         }
+    };
+    if constexpr (REC == 0) {
+        reference_recurrence();
     } else {
+        double r0[U], x0[U];
+#pragma unroll
+        for (int m = 0; m < U; m++) { r0[m] = r[m]; x0[m] = x[m]; }
         double w[U], wt[U], rw[U];
         double sigma = 0.0, rho_prev = 0.0, y_prev = 0.0;   /* y_prev: reciprocal estimate of rho_prev */
         for (int iter = 1; iter <= P.bicg_max_iter; iter++) {
@@ -569,6 +575,34 @@ __device__ __forceinline__ int bicg_iterate(const Sys<U, G>& S, const DeviceProb
             /* the update that used up the cap has not been tested yet */
             if (!exited && done > 0 && done == P.bicg_max_iter && grp_max_below<U, G>(S, ar, 1e-6)) exited = true;
         }
+        /* Safeguard: q is a recurrence, not a product, so r can drift from the
+         * true residual (and sigma can collapse).  The solution stands when every
+         * x is finite and the true residual b - A x passes the reference's exit
+         * test, or when the first rho test ended the solve (x = x_u, as in the
+         * reference's recurrence); otherwise the solve is redone from the start
+         * with the reference's recurrence. */
+        bool accept = exited;
+        if (accept) {
+            bool fin = true;
+#pragma unroll
+            for (int m = 0; m < U; m++) fin = fin && isfinite(x[m]);
+            accept = grp_all<U, G>(S, fin);
+        }
+        if (accept && done > 0) {
+            double ax[U], unused[U], zero[U], tr[U];
+#pragma unroll
+            for (int m = 0; m < U; m++) zero[m] = 0.0;
+            apply(x, zero, ax, unused, false);
+#pragma unroll
+            for (int m = 0; m < U; m++) tr[m] = fabs(b[m] - ax[m]);
+            accept = grp_max_below<U, G>(S, tr, 1e-6);
+        }
+        if (!accept) {
+            exited = false;
+#pragma unroll
+            for (int m = 0; m < U; m++) { r[m] = r0[m]; rt[m] = r0[m]; x[m] = x0[m]; p[m] = 0.0; pt[m] = 0.0; }
+            reference_recurrence();
+        }
     }
     if (!exited) capped = true;
     return done;
@@ -584,7 +618,7 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U, G>& S, const DeviceProbl
     constexpr int NMAX = WarpSmem<U, G>::NMAX;
     constexpr int LDW = WarpSmem<U, G>::LDW;
     const int N = S.N;
-    double xu[U], rd[U], r[U], x[U];
+    double xu[U], rd[U], r[U], x[U], bv[U];
     grp_sync(S);
 #pragma unroll
     for (int m = 0; m < U; m++) {
@@ -639,8 +673,10 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U, G>& S, const DeviceProbl
             double b = fma(rdm, (b0 + b1) + (b2 + b3), xu[m]);
             double ax = fma(rdm, (a0 + a1) + (a2 + a3), xu[m]);
             r[m] = b - ax;
+            bv[m] = b;
         } else {
             r[m] = 0.0;
+            bv[m] = 0.0;
         }
         x[m] = xu[m];
     }
@@ -681,7 +717,7 @@ __device__ __forceinline__ int coupled_rhs(const Sys<U, G>& S, const DeviceProbl
             }
         }
     };
-    const int done = bicg_iterate<U, G, REC>(S, P, r, x, apply, capped);
+    const int done = bicg_iterate<U, G, REC>(S, P, bv, r, x, apply, capped);
 #pragma unroll
     for (int m = 0; m < U; m++) F[m][IC] = x[m];
     return done;
@@ -753,11 +789,12 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
 #pragma unroll
     for (int j = 0; j < 32; j++) Wt[j * LDC + i] = wr[j];
     __syncwarp();
-    double r = 0.0;
+    double r = 0.0, bval = 0.0;
     if (valid) {
         const double b = fma(rd, (bs[0] + bs[1]) + (bs[2] + bs[3]), xu);
         const double ax = fma(rd, (as[0] + as[1]) + (as[2] + as[3]), xu);
         r = b - ax;
+        bval = b;
     }
     const double2* vp2 = reinterpret_cast<const double2*>(S.vp);
     const double2* vpt2 = reinterpret_cast<const double2*>(S.vpt);
@@ -792,7 +829,8 @@ __device__ __forceinline__ int coupled_rhs_regw(const Sys<1>& S, const DevicePro
         qto[0] = qt;
     };
     double rr[1] = {r}, xx[1] = {xu};
-    const int done = bicg_iterate<1, 1, REC>(S, P, rr, xx, apply, capped);
+    const double bb[1] = {bval};
+    const int done = bicg_iterate<1, 1, REC>(S, P, bb, rr, xx, apply, capped);
     const double x = xx[0];
     F[0][IC] = x;
     return done;
@@ -820,7 +858,7 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const Dev
     constexpr int H = NMAX / 2;
     const int N = S.N;
     /* with C = diag(a) G diag(b): x1 holds u = b X1sq (applied before G), rd holds v = rD a (after G) */
-    double xu[U], rd[U], x1[U], r[U], x[U];
+    double xu[U], rd[U], x1[U], r[U], x[U], bv[U];
     grp_sync(S);
 #pragma unroll
     for (int m = 0; m < U; m++) {
@@ -920,8 +958,10 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const Dev
             const double b = fma(rd[m], bsum[m], xu[m]);
             const double ax = fma(rd[m], asum[m], xu[m]);
             r[m] = b - ax;
+            bv[m] = b;
         } else {
             r[m] = 0.0;
+            bv[m] = 0.0;
         }
         x[m] = xu[m];
     }
@@ -976,7 +1016,7 @@ __device__ __forceinline__ int coupled_rhs_sharedc(const Sys<U, G>& S, const Dev
             qt[m] = vld ? fma(x1[m], qts[m], vt[m]) : 0.0;
         }
     };
-    const int done = bicg_iterate<U, G, REC>(S, P, r, x, apply, capped);
+    const int done = bicg_iterate<U, G, REC>(S, P, bv, r, x, apply, capped);
 #pragma unroll
     for (int m = 0; m < U; m++) F[m][IC] = x[m];
     return done;
@@ -1036,11 +1076,12 @@ __device__ __forceinline__ int coupled_rhs_regsym(const Sys<1>& S, const DeviceP
     };
     double bsum, asum;
     row_sums2(S.vcpt, S.vp, bsum, asum);
-    double r = 0.0;
+    double r = 0.0, bval = 0.0;
     if (valid) {
         const double b = fma(rd, bsum, xu);
         const double ax = fma(rd, asum, xu);
         r = b - ax;
+        bval = b;
     }
     /* q = A v = v + v_f (G (u v)), q~ = A^T vt = vt + u (G (v_f vt)) with u = b X1sq, v_f = rD a */
     auto apply = [&](const double (&v)[1], const double (&vt)[1], double (&qo)[1], double (&qto)[1], bool presynced) {
@@ -1054,7 +1095,8 @@ __device__ __forceinline__ int coupled_rhs_regsym(const Sys<1>& S, const DeviceP
         qto[0] = valid ? fma(x1, qts, vt[0]) : 0.0;
     };
     double rr[1] = {r}, xx[1] = {xu};
-    const int done = bicg_iterate<1, 1, REC>(S, P, rr, xx, apply, capped);
+    const double bb[1] = {bval};
+    const int done = bicg_iterate<1, 1, REC>(S, P, bb, rr, xx, apply, capped);
     const double x = xx[0];
     F[0][IC] = x;
     return done;
@@ -1104,7 +1146,7 @@ __device__ __forceinline__ int coupled_rhs_band(const Sys<1, G>& S, const Device
         for (int k = 0; k < UD; k++) F[0][k] = 0.0;
     }
     grp_sync(S);
-    double r = 0.0;
+    double r = 0.0, bval = 0.0;
     if (valid) {
         double bs[4] = {0.0, 0.0, 0.0, 0.0}, as[4] = {0.0, 0.0, 0.0, 0.0};
         int j = j0;
@@ -1119,6 +1161,7 @@ __device__ __forceinline__ int coupled_rhs_band(const Sys<1, G>& S, const Device
         const double b = fma(rd, (bs[0] + bs[1]) + (bs[2] + bs[3]), xu);
         const double ax = fma(rd, (as[0] + as[1]) + (as[2] + as[3]), xu);
         r = b - ax;
+        bval = b;
     }
     auto apply = [&](const double (&v)[1], const double (&vt)[1], double (&qo)[1], double (&qto)[1], bool presynced) {
         if (!presynced) grp_sync(S);
@@ -1142,7 +1185,8 @@ __device__ __forceinline__ int coupled_rhs_band(const Sys<1, G>& S, const Device
         qto[0] = qt;
     };
     double rr[1] = {r}, xx[1] = {xu};
-    const int done = bicg_iterate<1, G, REC>(S, P, rr, xx, apply, capped);
+    const double bb[1] = {bval};
+    const int done = bicg_iterate<1, G, REC>(S, P, bb, rr, xx, apply, capped);
     F[0][IC] = xx[0];
     return done;
 }

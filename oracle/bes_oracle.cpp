@@ -31,6 +31,7 @@
 #include "oracle_math.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -41,6 +42,8 @@
 
 namespace {
 
+/* solves of the single-reduction recurrence redone with the reference's (diagnostics) */
+std::atomic<long long> g_rec1_fallbacks{0};
 using std::fma;
 const int UD = BES_ORACLE_UD;
 const int NUP = BES_ORACLE_NUP;
@@ -117,13 +120,13 @@ inline double tree_max(const double* v, int n, double* tmp) {
 
 struct Work {
     int N;
-    std::vector<double> cpt, rd, x1sq, xu, b, r, rt, p, pt, q, qt, x, W, tmp, tmp2, us, vs, z, zt, wv, wtv;
+    std::vector<double> cpt, rd, x1sq, xu, b, r, rt, p, pt, q, qt, x, W, tmp, tmp2, us, vs, z, zt, wv, wtv, r0, tmp3;
     explicit Work(int n) : N(n) {
         int P = next_pow2_32(n);
         cpt.resize(n); rd.resize(n); x1sq.resize(n); xu.resize(n); b.resize(n);
         r.resize(n); rt.resize(n); p.resize(n); pt.resize(n); q.resize(n); qt.resize(n);
         x.resize(n); W.resize((size_t)n * n); tmp.resize(P); tmp2.resize(n); us.resize(n); vs.resize(n);
-        z.resize(n); zt.resize(n); wv.resize(n); wtv.resize(n);
+        z.resize(n); zt.resize(n); wv.resize(n); wtv.resize(n); r0.resize(n); tmp3.resize(n);
     }
 };
 
@@ -178,6 +181,7 @@ int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
                 acc = fma(C[i + (long)j * N] * w.x1sq[j], w.xu[j], acc);
             });
             ax = fma(w.rd[i], ax, w.xu[i]);
+            w.b[i] = bi;
             w.r[i] = bi - ax;
             w.rt[i] = w.r[i];
             w.x[i] = w.xu[i];
@@ -198,6 +202,7 @@ int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
             ax = row_sum4(N, [&](int j) { return C[i + (long)j * N] * w.x1sq[j]; }, [&](int j) { return w.xu[j]; });
             ax = fma(w.rd[i], ax, w.xu[i]);
         }
+        w.b[i] = bi;
         w.r[i] = bi - ax;
         w.rt[i] = w.r[i];
         w.x[i] = w.xu[i];
@@ -240,8 +245,8 @@ int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
     };
     int done = 0;
     bool exited = false;
-    if (variant == 0) {
-        /* the reference's recurrence, Steppers.cuh:508-561 */
+    /* the reference's recurrence, Steppers.cuh:508-561 */
+    auto reference_recurrence = [&]() {
         for (int i = 0; i < N; i++) w.tmp2[i] = w.r[i] * w.rt[i];
         double rho1 = tree_sum(w.tmp2.data(), N, w.tmp.data());
         double rho2 = 0.0;
@@ -272,6 +277,9 @@ int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
             for (int i = 0; i < N; i++) w.tmp2[i] = w.r[i] * w.rt[i];
             rho1 = tree_sum(w.tmp2.data(), N, w.tmp.data());
         }
+    };
+    if (variant == 0) {
+        reference_recurrence();
     } else {
         /* Single-reduction recurrence (the same iterates in exact arithmetic):
          * the products of the residuals w = A r, w~ = A^T r~ come first, then
@@ -283,7 +291,14 @@ int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
          * of p~.A p equal -rho/alpha_prev each by the biorthogonality of the
          * residuals, and rho/alpha_prev = beta sigma_prev).  The exits are the
          * reference's: |rho| < 1e-6 before the first update, max |r| < 1e-6
-         * after each update, at most max_iter updates. */
+         * after each update, at most max_iter updates.
+         * Its q is a recurrence, not a product, so r can drift from the true
+         * residual (and sigma can collapse): the solution is accepted only when
+         * every x is finite and the true residual b - A x passes the reference's
+         * exit test (max < 1e-6), or when the first rho test ended the solve;
+         * otherwise the solve is redone from the start with the reference's
+         * recurrence. */
+        for (int i = 0; i < N; i++) w.r0[i] = w.r[i];
         double sigma = 0.0, rho_prev = 0.0;
         for (int iter = 1; iter <= max_iter; iter++) {
             apply(w.r.data(), w.rt.data(), w.wv.data(), w.wtv.data());
@@ -318,6 +333,22 @@ int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
             const double rmax = tree_max(w.tmp2.data(), N, w.tmp.data());
             done++;
             if (rmax < 1e-6) { exited = true; break; }
+        }
+        /* an exit at the first rho test leaves x = x_u, as the reference's recurrence does */
+        bool accept = exited;
+        for (int i = 0; i < N && accept; i++) accept = std::isfinite(w.x[i]);
+        if (accept && done > 0) {
+            /* true residual b - A x (the second product's result is not used) */
+            for (int i = 0; i < N; i++) w.tmp3[i] = 0.0;
+            apply(w.x.data(), w.tmp3.data(), w.wv.data(), w.wtv.data());
+            for (int i = 0; i < N; i++) w.tmp2[i] = std::fabs(w.b[i] - w.wv[i]);
+            accept = tree_max(w.tmp2.data(), N, w.tmp.data()) < 1e-6;
+        }
+        if (!accept) {
+            g_rec1_fallbacks++;
+            exited = false;
+            for (int i = 0; i < N; i++) { w.r[i] = w.r0[i]; w.rt[i] = w.r0[i]; w.x[i] = w.xu[i]; }
+            reference_recurrence();
         }
     }
     *capped = !exited;
@@ -712,6 +743,12 @@ int bes_oracle_rhs(int n, double t, const double* state, const double* upar,
     Work w(n);
     bool capped = false;
     return coupled_rhs(w, t, state, state + n, upar, n, coupling, bicg_max_iter, f, f + n, &capped);
+}
+
+long long bes_oracle_rec1_fallbacks(int reset) {
+    const long long v = g_rec1_fallbacks.load();
+    if (reset) g_rec1_fallbacks = 0;
+    return v;
 }
 
 int bes_oracle_max_threads(void) {

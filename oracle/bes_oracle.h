@@ -120,6 +120,10 @@ int bes_oracle_rhs(int n, double t, const double* state, const double* upar,
 
 int bes_oracle_max_threads(void);
 
+/* number of single-reduction BiCG solves redone with the reference's
+ * recurrence since the last reset (reset != 0 clears it) */
+long long bes_oracle_rec1_fallbacks(int reset);
+
 #ifdef __cplusplus
 }
 #endif

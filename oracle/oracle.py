@@ -72,6 +72,8 @@ def lib() -> ctypes.CDLL:
         L.bes_oracle_rhs.argtypes = [ctypes.c_int, ctypes.c_double, _dp, _dp, _dp, ctypes.c_int, _dp]
         L.bes_oracle_rhs.restype = ctypes.c_int
         L.bes_oracle_max_threads.restype = ctypes.c_int
+        L.bes_oracle_rec1_fallbacks.argtypes = [ctypes.c_int]
+        L.bes_oracle_rec1_fallbacks.restype = ctypes.c_longlong
         _lib = L
     return _lib
 
