@@ -74,7 +74,8 @@ def test_matches_reference_golden(gpu, name):
     golden_compare.check(name, got)
 
 
-@pytest.mark.parametrize("name", ["c1_n32", "cloud_n64", "cloud_n128"])
+@pytest.mark.parametrize("name", [n for n in ("c1_n32", "cloud_n64", "cloud_n128", "c1_n32_4p")
+                                  if n in cases.AVAILABLE])
 def test_factored_matches_reference_golden(gpu, name):
     ens, run = cases.build(name, factored=True)
     got = run_gpu(ens, n_periods=run["n_periods"], reset_at=run["reset_at"], bicg_recurrence=REC)

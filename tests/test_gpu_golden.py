@@ -16,7 +16,8 @@ def test_kernel_matches_reference_golden(name, gpu):
     golden_compare.check(name, got)
 
 
-@pytest.mark.parametrize("name", ["c1_n32", "cloud_n64", "cloud_n128"])
+@pytest.mark.parametrize("name", [n for n in ("c1_n32", "cloud_n64", "cloud_n128", "c1_n32_4p")
+                                  if n in cases.AVAILABLE])
 def test_symmetric_geometry_kernels_match_reference_golden(name, gpu):
     """The same systems as a shared symmetric geometry with unit factors (row of
     G in registers for N = 32, one shared-memory read for both products above)
