@@ -148,6 +148,8 @@ def parse():
                     help="c1_period1 coupling input: the symmetric line geometry 1/d shared by the launch with unit "
                          "factors R^-2, R^3 (default; the same matrix R_j^3/(R_i^2 d_ij) as a product) or the "
                          "reference-format matrix itself")
+    ap.add_argument("--horizon", type=int, default=1, choices=[0, 1],
+                    help="c1_period1: also time configuration 1's 64-period horizon (c1_full) in the same line")
     ap.add_argument("--ring-full", action="store_true",
                     help="ring_period1: solve the banded matrices through the full-matrix operator")
     ap.add_argument("--autotune", type=int, default=1, choices=[0, 1],
@@ -465,9 +467,56 @@ def run_b200(args, rank, world, local):
     if world == 1 and args.workload == "c1_period1" and args.c1_format == "geometry":
         # like for like with the reference arm: the same ensemble with the reference-format matrix as input
         line["reference_format_input"] = reference_format_steps(args, local, flush)
+    if world == 1 and args.workload == "c1_period1" and args.horizon:
+        # configuration 1's own horizon: 64 periods with the accessory reset before period 33
+        line["c1_full"] = horizon_steps(args, local, flush)
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(ens, args.cpu_sample_systems)
     return line
+
+
+def horizon_steps(args, local, flush):
+    """c1_full (the same 256 systems, 64 periods, accessories reset before period 33, step budget 20000 per
+    period): one untimed warm-up step and one timed step, device-resident."""
+    import torch
+
+    from bubbleensemble_implicitextension_b200 import solver as S
+    V = S.ListOfVariables
+    ens = make_ensemble("c1_full")
+    ens.max_steps_per_period = STEP_BUDGET["c1_full"]
+    n_per, reset_at = PERIODS["c1_full"]
+    ps = ens.make_solver(device=local)
+    try:
+        ps.SolverOption(S.ListOfSolverOptions.BiCGRecurrence, args.bicg_recurrence)
+        stream = torch.cuda.current_stream()
+        ps.set_stream(stream.cuda_stream)
+        ps.SynchroniseFromHostToDevice(V.All)
+        torch.cuda.synchronize()
+        times = []
+        for it in range(2):
+            ps.SynchroniseFromHostToDevice(V.ActualState)
+            ps.SynchroniseFromHostToDevice(V.UnitAccessories)
+            ps.SynchroniseFromHostToDevice(V.IntegerUnitAccessories)
+            ps.reset_counters()
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ps.solve_periods(n_per, reset_at)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        ps.SynchroniseFromDeviceToHost(V.Counters)
+        ps.InsertSynchronisationPoint()
+        ps.SynchroniseSolver()
+        c = ps.counters()
+    finally:
+        ps.close()
+    ms = times[-1]
+    done = int(((c["status"] & 4) == 0).sum())
+    return {"value": ens.n_systems * n_per / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "warmup": 1, "steps": 1,
+            "periods_per_step": n_per, "systems_at_step_budget": int(ens.n_systems - done),
+            "completed_system_periods_per_s": done * n_per / (ms * 1e-3),
+            "status_or": int(np.bitwise_or.reduce(c["status"])), "workload": WORKLOADS["c1_full"]}
 
 
 def reference_format_steps(args, local, flush):
