@@ -257,12 +257,14 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def flops_per_system(n, attempted, bicg):
+def flops_per_system(n, attempted, bicg, band=0):
     """Algorithmic FP64 flops (FMA = 2): per attempted RKCK45 step 6 right-hand sides of
     55N (Keller-Miksis) + 5N^2 + 5N (b and the first residual) plus 110N (stages and
-    controller); per completed BiCG iteration 6N^2 + 17N."""
-    rhs_base = 55 * n + 5 * n * n + 5 * n
-    return attempted * (6 * rhs_base + 110 * n) + bicg * (6 * n * n + 17 * n)
+    controller); per completed BiCG iteration 6N^2 + 17N.  With banded storage (band =
+    CBW > 0) every N^2 becomes N * min(2 CBW + 1, N), the entries the products read."""
+    nn = n * min(2 * band + 1, n) if band > 0 else n * n
+    rhs_base = 55 * n + 5 * nn + 5 * n
+    return attempted * (6 * rhs_base + 110 * n) + bicg * (6 * nn + 17 * n)
 
 
 def read_traffic():
@@ -376,7 +378,8 @@ def run_b200(args, rank, world, local):
     ps.SynchroniseSolver()
     c = ps.counters()
     attempted = (c["accepted"] + c["rejected"]).astype(np.float64)
-    flops = float(sum(flops_per_system(int(n), a, b) for n, a, b in zip(ens.units, attempted, c["bicg"].astype(np.float64))))
+    flops = float(sum(flops_per_system(int(n), a, b, int(ens.band_width))
+                      for n, a, b in zip(ens.units, attempted, c["bicg"].astype(np.float64))))
     total_ms = sum(times)
     max_ms = allreduce_max(total_ms, world)
     ms_per_step = max_ms / args.steps
