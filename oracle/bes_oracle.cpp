@@ -44,6 +44,7 @@ namespace {
 
 /* solves of the single-reduction recurrence redone with the reference's (diagnostics) */
 std::atomic<long long> g_rec1_fallbacks{0};
+std::atomic<long long> g_rec1_fallback_capped{0};
 using std::fma;
 const int UD = BES_ORACLE_UD;
 const int NUP = BES_ORACLE_NUP;
@@ -346,6 +347,7 @@ int coupled_rhs(Work& w, double T, const double* y0, const double* y1,
         }
         if (!accept) {
             g_rec1_fallbacks++;
+            if (!exited) g_rec1_fallback_capped++;
             exited = false;
             for (int i = 0; i < N; i++) { w.r[i] = w.r0[i]; w.rt[i] = w.r0[i]; w.x[i] = w.xu[i]; }
             reference_recurrence();
@@ -748,6 +750,12 @@ int bes_oracle_rhs(int n, double t, const double* state, const double* upar,
 long long bes_oracle_rec1_fallbacks(int reset) {
     const long long v = g_rec1_fallbacks.load();
     if (reset) g_rec1_fallbacks = 0;
+    return v;
+}
+
+long long bes_oracle_rec1_fallbacks_capped(int reset) {
+    const long long v = g_rec1_fallback_capped.load();
+    if (reset) g_rec1_fallback_capped = 0;
     return v;
 }
 

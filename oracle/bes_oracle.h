@@ -123,6 +123,8 @@ int bes_oracle_max_threads(void);
 /* number of single-reduction BiCG solves redone with the reference's
  * recurrence since the last reset (reset != 0 clears it) */
 long long bes_oracle_rec1_fallbacks(int reset);
+/* of those, the solves the iteration cap ended */
+long long bes_oracle_rec1_fallbacks_capped(int reset);
 
 #ifdef __cplusplus
 }

@@ -74,6 +74,8 @@ def lib() -> ctypes.CDLL:
         L.bes_oracle_max_threads.restype = ctypes.c_int
         L.bes_oracle_rec1_fallbacks.argtypes = [ctypes.c_int]
         L.bes_oracle_rec1_fallbacks.restype = ctypes.c_longlong
+        L.bes_oracle_rec1_fallbacks_capped.argtypes = [ctypes.c_int]
+        L.bes_oracle_rec1_fallbacks_capped.restype = ctypes.c_longlong
         _lib = L
     return _lib
 
