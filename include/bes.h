@@ -105,9 +105,12 @@ typedef int32_t bes_status;
 #define BES_OPT_BICG_RECURRENCE 105        /* 0 (default): the reference's BiCG recurrence (Steppers.cuh:508-561:
                                               two reductions per iteration); 1: the single-reduction form of the
                                               same iterates (residual products first, rho = r.r~ and mu = r~.Ar
-                                              in one reduction, sigma = mu - beta^2 sigma_prev).  Equal in exact
-                                              arithmetic, rounded differently: results stay within the parity
-                                              tolerances of the reference, not bit-identical to option 0. */
+                                              in one reduction, sigma = mu - beta^2 sigma_prev).  A solve of form
+                                              1 stands only if x is finite and the true residual b - A x passes
+                                              the reference's exit test; otherwise (and at the iteration cap) it
+                                              is redone with form 0.  Equal in exact arithmetic, rounded
+                                              differently: results stay within the parity tolerances of the
+                                              reference, not bit-identical to option 0. */
 
 /* Algorithms, Interface.cuh:33 */
 #define BES_RK4 0
