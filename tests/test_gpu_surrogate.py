@@ -81,4 +81,45 @@ def test_screened_sweep_integrates_fewer_points_at_bounded_error(gpu):
     np.testing.assert_array_equal(res.map[res.integrated], plain[res.integrated])
     served = ~res.integrated
     err = np.abs(res.map[served][:, 0] - plain[served][:, 0])
-    assert np.median(err) < 0.15                                 # log10 strength, served points
+    print("integrated fraction", frac, "median log10 strength error of served points", float(np.median(err)))
+    assert np.median(err) < 0.08                                 # log10 strength (20 % relative), served points
+
+
+def test_lattice_screener_with_and_without_network(gpu):
+    """The multi-fidelity sweep screener with the trained network and without it
+    (bilinear interpolation of the solver lattice, the counterfactual): both
+    reproduce the solver exactly where they integrate and serve the rest within a
+    bounded error; the network's map is not worse than plain interpolation.  On
+    the benchmark's sweep (128 x 128 points, 8 periods) the two served maps came
+    out equal (mean error 1.68 % both): the network gains nothing measurable
+    there, which this test does not hide -- it asserts no gain, only no loss."""
+    radii = np.random.default_rng(11).uniform(2.0, 8.0, 32)
+    X, Y, status, _ = SG.generate_runs(768, seed=3, n_periods=2, reset_at=1)
+    ok = (status & 4) == 0
+    net = SG.MLP(max_batch=1024, seed=2)
+    net.fit(X[ok], Y[ok], steps=2000, batch=256, lr=2e-3)
+    n = 33
+    pa = np.linspace(0.5, 2.0, n)
+    fr = np.logspace(np.log10(20.0), np.log10(200.0), n)
+
+    def solve(pa_pts, f_pts):
+        ens = SG.line_ensemble(pa_pts, f_pts, np.broadcast_to(radii, (len(pa_pts), 32)), n_periods=2, reset_at=1)
+        return SG.solve_ensemble(ens)[0]
+
+    PA, FR = np.meshgrid(pa, fr, indexing="ij")
+    plain = solve(PA.ravel(), FR.ravel()).reshape(n, n, 2)
+    stats = {}
+    for tag, m in (("network", net), ("interpolation", None)):
+        res = SG.screen_sweep_lattice(m, pa, fr, radii, solve, stride=4, cell_spread=0.3, cell_disagreement=0.1,
+                                      audit_fraction=0.02)
+        np.testing.assert_array_equal(res.map[res.integrated], plain[res.integrated])
+        served = ~res.integrated
+        assert served.any(), tag
+        e = np.abs(10.0 ** res.map[..., 0] - 10.0 ** plain[..., 0]) / 10.0 ** plain[..., 0]
+        stats[tag] = (float(res.integrated.mean()), float(np.median(e[served])), float(e[served].mean()))
+    print("integrated fraction, median and mean served strength error:", stats)
+    net.close()
+    for tag, (frac, med, mean) in stats.items():
+        assert frac < 0.9, (tag, stats)
+        assert med < 0.10, (tag, stats)           # collapse strength, relative
+    assert stats["network"][2] <= 1.5 * stats["interpolation"][2] + 0.01, stats
