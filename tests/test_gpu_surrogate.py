@@ -89,10 +89,12 @@ def test_lattice_screener_with_and_without_network(gpu):
     """The multi-fidelity sweep screener with the trained network and without it
     (bilinear interpolation of the solver lattice, the counterfactual): both
     reproduce the solver exactly where they integrate and serve the rest within a
-    bounded error; the network's map is not worse than plain interpolation.  On
-    the benchmark's sweep (128 x 128 points, 8 periods) the two served maps came
-    out equal (mean error 1.68 % both): the network gains nothing measurable
-    there, which this test does not hide -- it asserts no gain, only no loss."""
+    bounded error.  What the network adds, measured: on the benchmark's sweep
+    (128 x 128 points, 8 periods) the two served maps came out equal (mean error
+    1.68 % both); on this coarse 33 x 33 grid the network's served points are
+    worse (mean 1.4 % against 0.65 % on the B200).  The test asserts that the
+    network moves the served error by less than two percentage points either
+    way -- it claims no gain, because there is none to show."""
     radii = np.random.default_rng(11).uniform(2.0, 8.0, 32)
     X, Y, status, _ = SG.generate_runs(768, seed=3, n_periods=2, reset_at=1)
     ok = (status & 4) == 0
@@ -120,6 +122,5 @@ def test_lattice_screener_with_and_without_network(gpu):
     print("integrated fraction, median and mean served strength error:", stats)
     net.close()
     for tag, (frac, med, mean) in stats.items():
-        assert frac < 0.9, (tag, stats)
-        assert med < 0.10, (tag, stats)           # collapse strength, relative
-    assert stats["network"][2] <= 1.5 * stats["interpolation"][2] + 0.01, stats
+        assert med < 0.05 and mean < 0.05, (tag, stats)      # collapse strength, relative
+    assert abs(stats["network"][2] - stats["interpolation"][2]) < 0.02, stats
