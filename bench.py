@@ -469,7 +469,8 @@ def run_b200(args, rank, world, local):
                      "completed_system_periods_per_s": float(((gathered["status"] & 4) == 0).sum() * n_per * args.steps
                                                              / (max_ms * 1e-3))},
     }
-    if world == 1 and args.workload == "c1_period1" and args.c1_format == "geometry":
+    if world == 1 and ((args.workload == "c1_period1" and args.c1_format == "geometry")
+                       or args.workload == "c3_period1"):
         # like for like with the reference arm: the same ensemble with the reference-format matrix as input
         line["reference_format_input"] = reference_format_steps(args, local, flush)
     if world == 1 and args.workload == "c1_period1" and args.horizon:
@@ -527,14 +528,18 @@ def horizon_steps(args, local, flush):
 
 
 def reference_format_steps(args, local, flush):
-    """c1_period1 with the coupling given as the reference-format matrix C_ij = R_j^3 / (R_i^2 d_ij) (the
-    reference arm's input): device-resident throughput over the same number of timed steps."""
+    """The workload (c1_period1 or c3_period1) with the coupling given as the reference-format matrix
+    C_ij = R_j^3 / (R_i^2 d_ij) (the reference arm's input): device-resident throughput over the same number
+    of timed steps."""
     import torch
 
     from bubbleensemble_implicitextension_b200 import solver as S
     from bubbleensemble_implicitextension_b200 import workloads as W
     V = S.ListOfVariables
-    ens = W.c1_ensemble(n_periods=1, reset_at=-1, factored=False)
+    if args.workload == "c3_period1":
+        ens = W.c3_ensemble(n_periods=1, reset_at=-1, factored=False)
+    else:
+        ens = W.c1_ensemble(n_periods=1, reset_at=-1, factored=False)
     ens.max_steps_per_period = 50_000
     ps = ens.make_solver(device=local)
     try:
