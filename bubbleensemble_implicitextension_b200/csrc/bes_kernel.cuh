@@ -540,14 +540,27 @@ __device__ __forceinline__ int bicg_iterate(const Sys<U, G>& S, const DeviceProb
             for (int m = 0; m < U; m++) { prod[m] = r[m] * rt[m]; rw[m] = rt[m] * w[m]; }
             double rho, mu;
             grp_tree_sum2<U, G>(S, prod, rw, rho, mu);
+            double alpha;
             if (iter == 1) {
                 if (fabs(rho) < 1e-6) { exited = true; break; }
 #pragma unroll
                 for (int m = 0; m < U; m++) { p[m] = r[m]; pt[m] = rt[m]; q[m] = w[m]; qt[m] = wt[m]; }
                 sigma = mu;
+                alpha = math::div_known(rho, sigma, math::recip_estimate(sigma));   /* = rho / sigma */
             } else {
-                const double beta = math::div_known(rho, rho_prev, y_prev);   /* = rho / rho_prev */
-                sigma = fma(-(beta * beta), sigma, mu);
+                /* beta = rho / rho_prev: sigma and alpha go on from Markstein's quotient
+                 * while its proof runs; an unproven quotient redoes them from the IEEE
+                 * one, so both are always the correctly rounded values */
+                bool beta_ok;
+                double beta = math::div_markstein(rho, rho_prev, y_prev, beta_ok);
+                double sg = fma(-(beta * beta), sigma, mu);
+                alpha = math::div_known(rho, sg, math::recip_estimate(sg));   /* = rho / sigma */
+                if (__builtin_expect(!beta_ok, 0)) {
+                    beta = math::div_ieee(rho, rho_prev);
+                    sg = fma(-(beta * beta), sigma, mu);
+                    alpha = math::div_known(rho, sg, math::recip_estimate(sg));
+                }
+                sigma = sg;
 #pragma unroll
                 for (int m = 0; m < U; m++) {
                     p[m] = fma(beta, p[m], r[m]);
@@ -556,7 +569,6 @@ __device__ __forceinline__ int bicg_iterate(const Sys<U, G>& S, const DeviceProb
                     qt[m] = fma(beta, qt[m], wt[m]);
                 }
             }
-            const double alpha = math::div_known(rho, sigma, math::recip_estimate(sigma));   /* = rho / sigma */
             rho_prev = rho;
             y_prev = math::recip_estimate(rho);
 #pragma unroll

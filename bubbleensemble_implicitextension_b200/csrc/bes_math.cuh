@@ -56,30 +56,34 @@ __device__ __forceinline__ double pow2_scale(double x, int k) {
 
 /* ---------------------------------------------------------------------------
  * Division by a divisor known ahead of time.  recip_estimate(b) is the
- * hardware's approximate reciprocal refined by two Newton-Raphson steps
- * y <- y + y (1 - b y), within about an ulp of 1/b for normal b, with no
- * branches, so it can be computed off the critical path as soon as b is known.
- * div_known(a, b, y) then forms the quotient by Markstein's correction
- * q1 = q0 + (a - b q0) y, q0 = a y (P. Markstein, IBM J. Res. Dev. 34 (1990)
- * 111-119), and accepts q1 only when the exact remainder r1 = a - b q1 (one
- * fma) proves it to be the rounded quotient: |r1| < ulp(q1)/2 |b| with q1 not
- * a power of two (so the ulp is the same on both sides of q1) and a, b within
- * [2^-400, 2^400] (no overflow, underflow or subnormal along the way).
- * Otherwise the IEEE division decides.  The result is therefore always the
- * correctly rounded a / b. */
+ * hardware's approximate reciprocal refined by one Newton-Raphson step
+ * y <- y + y (1 - b y), with no branches, so it can be computed off the
+ * critical path as soon as b is known.  div_markstein(a, b, y, ok) then forms
+ * the quotient by Markstein's correction q1 = q0 + (a - b q0) y, q0 = a y
+ * (P. Markstein, IBM J. Res. Dev. 34 (1990) 111-119): the Newton step
+ * squares the relative error of the hardware estimate and the correction
+ * squares that of y again, so q1 is the rounded quotient unless a / b lies
+ * very close to a rounding boundary.
+ * ok reports the proof that it is: the exact remainder r1 = a - b q1 (one
+ * fma) satisfies |r1| < ulp(q1)/2 |b|, with q1 not a power of two (so the ulp
+ * is the same on both sides of q1) and a, b within [2^-400, 2^400] (no
+ * overflow, underflow or subnormal along the way).  The test is sound for any
+ * y: rounding is monotonic and ulp(q1)/2 |b| is exact, so a rounded remainder
+ * below the bound means the exact one is.  A caller may go on with q1 before
+ * ok is known and redo the work that used it when ok is false, which keeps
+ * the test off its dependency chain.  div_known(a, b, y) returns q1 when ok
+ * and the IEEE quotient otherwise; both therefore always give the correctly
+ * rounded a / b. */
 __device__ __forceinline__ double recip_estimate(double b) {
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
-    double e = fma(-b, y, 1.0);
-    y = fma(y, e, y);
-    e = fma(-b, y, 1.0);
-    y = fma(y, e, y);
-    return y;
+    const double e = fma(-b, y, 1.0);
+    return fma(y, e, y);
 }
 
 static __device__ __noinline__ double div_ieee(double a, double b) { return a / b; }
 
-__device__ __forceinline__ double div_known(double a, double b, double y) {
+__device__ __forceinline__ double div_markstein(double a, double b, double y, bool& ok) {
     const double q0 = a * y;
     const double r0 = fma(-q0, b, a);
     const double q1 = fma(r0, y, q0);
@@ -87,8 +91,14 @@ __device__ __forceinline__ double div_known(double a, double b, double y) {
     const long long qb = __double_as_longlong(q1);
     const double half_ulp_b = __longlong_as_double(qb & 0x7ff0000000000000LL) * 0x1p-53 * fabs(b);
     const double aa = fabs(a), ab = fabs(b);
-    const bool ok = aa >= 0x1p-400 && aa <= 0x1p400 && ab >= 0x1p-400 && ab <= 0x1p400 &&
-                    (qb & 0x000fffffffffffffLL) != 0 && fabs(r1) < half_ulp_b;
+    ok = aa >= 0x1p-400 && aa <= 0x1p400 && ab >= 0x1p-400 && ab <= 0x1p400 &&
+         (qb & 0x000fffffffffffffLL) != 0 && fabs(r1) < half_ulp_b;
+    return q1;
+}
+
+__device__ __forceinline__ double div_known(double a, double b, double y) {
+    bool ok;
+    const double q1 = div_markstein(a, b, y, ok);
     if (__builtin_expect(!ok, 0)) return div_ieee(a, b);
     return q1;
 }

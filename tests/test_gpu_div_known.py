@@ -5,7 +5,10 @@ oracle.  A small probe program built from csrc/bes_math.cuh compares the bits
 of both on the GPU over 2^26 operand pairs per family: random bit patterns
 (every exponent, zeros, subnormals, infinities, NaNs), operands of the sizes
 the BiCG sums take (|x| in 2^-60 .. 2^60), divisors that are powers of two,
-and quotients near powers of two."""
+and quotients near powers of two.  It also checks that math::div_markstein
+never reports a quotient as proven that is not the IEEE one, and that on
+operands of the BiCG sums' sizes it leaves few quotients unproven (each of
+those costs the IEEE division on top of the corrected one)."""
 import shutil
 import subprocess
 from pathlib import Path
@@ -32,7 +35,7 @@ __device__ double in_range(uint64_t r, int lo, int hi) {
     return __longlong_as_double((long long)(((r >> 12) & 0x000fffffffffffffull) | (e << 52) | ((r >> 11) & 1ull) << 63));
 }
 __global__ void probe(int family, uint64_t n, unsigned long long* bad) {
-    unsigned long long nb = 0;
+    unsigned long long nb = 0, wrong_ok = 0, unproven = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t r1 = mix(2 * i + 1 + ((uint64_t)family << 40)), r2 = mix(2 * i + 2 + ((uint64_t)family << 40));
         double a, b;
@@ -45,18 +48,25 @@ __global__ void probe(int family, uint64_t n, unsigned long long* bad) {
         const double got = bes::math::div_known(a, b, bes::math::recip_estimate(b));
         const bool same = __double_as_longlong(got) == __double_as_longlong(want) || (isnan(got) && isnan(want));
         if (!same) nb++;
+        bool ok;
+        const double q1 = bes::math::div_markstein(a, b, bes::math::recip_estimate(b), ok);
+        if (ok && __double_as_longlong(q1) != __double_as_longlong(want)) wrong_ok++;
+        if (!ok) unproven++;
     }
     atomicAdd(bad, nb);
+    atomicAdd(bad + 1, wrong_ok);
+    atomicAdd(bad + 2, unproven);
 }
 int main() {
     unsigned long long* bad;
-    if (cudaMallocManaged(&bad, 8) != cudaSuccess) { std::printf("cuda error\n"); return 2; }
+    if (cudaMallocManaged(&bad, 24) != cudaSuccess) { std::printf("cuda error\n"); return 2; }
     const uint64_t n = 1ull << 26;
     for (int f = 0; f < 4; f++) {
-        *bad = 0;
+        bad[0] = bad[1] = bad[2] = 0;
         probe<<<148 * 8, 256>>>(f, n, bad);
         if (cudaDeviceSynchronize() != cudaSuccess) { std::printf("cuda error\n"); return 2; }
-        std::printf("family %d pairs %llu mismatches %llu\n", f, (unsigned long long)n, *bad);
+        std::printf("family %d pairs %llu unproven %llu proven_wrong %llu mismatches %llu\n", f,
+                    (unsigned long long)n, bad[2], bad[1], bad[0]);
     }
     return 0;
 }
@@ -75,5 +85,10 @@ def test_div_known_equals_ieee_division(tmp_path, gpu):
     assert out.returncode == 0, out.stdout + out.stderr
     lines = [l for l in out.stdout.splitlines() if l.startswith("family")]
     assert len(lines) == 4, out.stdout
+    print(out.stdout)
     for line in lines:
-        assert line.endswith("mismatches 0"), out.stdout
+        assert line.endswith("proven_wrong 0 mismatches 0"), out.stdout
+    # operands of the sizes the BiCG sums take: the corrected quotient is proven
+    # for all but a small share (a high share would mean a poor estimate)
+    f1 = lines[1].split()
+    assert int(f1[f1.index("unproven") + 1]) < (1 << 26) // 1000, out.stdout
