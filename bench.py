@@ -784,7 +784,7 @@ def run_strip(args, rank, world, local):
             "strip": out, "gpu_launches": None}
 
 
-# the recurrence measured faster per workload (B200, this build): c1_period1 381 vs 418 ms per step with
+# the recurrence measured faster per workload (on a B200): c1_period1 377 vs 412 ms per step with
 # 1 and 0; c3_period1 4351 vs 4079 ms; c2_period1 and c1_full are set by systems whose solves often reach
 # the iteration cap, which the single-reduction form's safeguard redoes with the reference's recurrence
 FASTER_RECURRENCE = {"c1_period1": 1}
